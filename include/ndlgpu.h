@@ -1,0 +1,202 @@
+/*
+ * ndlgpu.h -- C ABI of the B200 separable-convolution library (libndlgpu.so).
+ *
+ * Drop-in boundary for ndl's convolution hot path.  Every entry point below
+ * replaces one reference interface; the citation is given per function
+ * (paths relative to the ndl source tree).  The reference is a header-only
+ * C++17 template library, so its "interface" is the template signature; the
+ * C++ overloads in ndlgpu_dropin.h rebuild exactly those signatures on top of
+ * this ABI.
+ *
+ * Conventions
+ *   - Plain C: no C++ or torch types cross this boundary.  Status codes, never
+ *     exceptions.  ndlgpu_last_error() gives a per-thread detail message.
+ *   - Images are views {data, dtype, rank, extent[], stride[]} in ndl axis
+ *     order (axis 0 fastest for a default layout, image/core.h:858-864),
+ *     strides signed and in ELEMENTS -- exactly the triple an ndl::Image<T,DIM>
+ *     carries after view()/slice()/swap_axes()/mirror() (image/core.h:50-972),
+ *     with `data` = &image.at({0,..,0}).  Image data lives in device memory.
+ *   - All work is asynchronous on the given CUDA stream (a cudaStream_t passed
+ *     as void*; NULL = legacy default stream).  Host arrays given as arguments
+ *     (kernels, sigmas, tap lists) are copied before the call returns.
+ *   - Validation happens on the host, before any CUDA call: a call that
+ *     returns an error has enqueued nothing.
+ */
+#ifndef NDLGPU_H
+#define NDLGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define NDLGPU_API __attribute__((visibility("default")))
+#else
+#define NDLGPU_API
+#endif
+
+#define NDLGPU_MAX_RANK 8
+/* Largest number of taps of one 1-D axis kernel (the fused kernels handle up
+ * to 37 taps per axis, sigma = 6; longer kernels run the general kernels). */
+#define NDLGPU_MAX_TAPS 255
+/* Largest number of nonzero taps of a full N-D kernel given to
+ * ndlgpu_convolve() (the non-separable general path). */
+#define NDLGPU_MAX_ND_TAPS 4096
+
+typedef enum ndlgpu_status {
+    NDLGPU_OK = 0,
+    NDLGPU_ERR_INVALID_ARGUMENT = 1,     /* null pointer, rank, axis, negative extent, ... */
+    NDLGPU_ERR_UNSUPPORTED_DTYPE = 2,
+    NDLGPU_ERR_EXTENT_MISMATCH = 3,      /* dst.extent != src.extent (convolution.h:59) */
+    NDLGPU_ERR_RADIUS_EXCEEDS_EXTENT = 4,/* Wrap/Reflect tap beyond one period (mathHelpers.h:23-24) */
+    NDLGPU_ERR_ALIASING = 5,             /* src and dst memory ranges overlap */
+    NDLGPU_ERR_INDEX_OVERFLOW = 6,       /* a view spans more than 2^62 elements */
+    NDLGPU_ERR_BAD_SIGMA = 7,            /* sigma <= 0 or not finite (convolution.h:112) */
+    NDLGPU_ERR_WORKSPACE = 8,            /* caller workspace smaller than required */
+    NDLGPU_ERR_CUDA = 9,                 /* a CUDA runtime call failed */
+    NDLGPU_ERR_OUT_OF_MEMORY = 10,
+    NDLGPU_ERR_TOO_MANY_TAPS = 11,
+    NDLGPU_ERR_DEVICE_CHECK = 12         /* a kernel's own guard fired (see ndlgpu_device_status) */
+} ndlgpu_status;
+
+/* Element types.  bf16/f16 have no ndl counterpart (ndl accepts any
+ * arithmetic T, convolution.h:57-58); they are storage formats here. */
+typedef enum ndlgpu_dtype {
+    NDLGPU_U8 = 0, NDLGPU_I8 = 1, NDLGPU_U16 = 2, NDLGPU_I16 = 3,
+    NDLGPU_I32 = 4, NDLGPU_U32 = 5, NDLGPU_I64 = 6, NDLGPU_U64 = 7,
+    NDLGPU_F32 = 8, NDLGPU_F64 = 9, NDLGPU_F16 = 10, NDLGPU_BF16 = 11
+} ndlgpu_dtype;
+
+/* Same order as ndl::BorderMode (image/border_mode.h:14-19). */
+typedef enum ndlgpu_border {
+    NDLGPU_CLAMP = 0, NDLGPU_WRAP = 1, NDLGPU_REFLECT = 2
+} ndlgpu_border;
+
+/* How a chain of 1-D passes turns into DstT.
+ *  ROUND_ONCE: gaussian_blur()'s structure (convolution.h:148-185): passes
+ *    accumulate without intermediate rounding; one final conversion, which
+ *    is std::round (half away from zero) for integral DstT.  A single pass
+ *    is a plain convolve() (truncating cast), as gaussian_blur()'s DIM==1
+ *    branch (convolution.h:141-146).
+ *  CAST_EACH: every pass is a complete convolve() into DstT (truncating for
+ *    integral DstT, convolution.h:69) -- the chain a caller gets by calling
+ *    convolve() once per axis. */
+typedef enum ndlgpu_compose {
+    NDLGPU_ROUND_ONCE = 0, NDLGPU_CAST_EACH = 1
+} ndlgpu_compose;
+
+/* Arithmetic.  AUTO: integral DstT and f64 data are computed bit-exactly
+ * (integer arithmetic when every tap is a dyadic fraction, otherwise the
+ * reference's own double sequence: each tap multiplied then added in
+ * convolve()'s tap order, convolution.h:66-68); f32/f16/bf16 DstT accumulate
+ * in FP32.  FP32: force FP32 accumulation.  EXACT: force the bit-exact
+ * double sequence for every type (slower). */
+typedef enum ndlgpu_precision {
+    NDLGPU_PREC_AUTO = 0, NDLGPU_PREC_FP32 = 1, NDLGPU_PREC_EXACT = 2
+} ndlgpu_precision;
+
+typedef struct ndlgpu_view {
+    void* data;                         /* &at({0,...,0}) */
+    int32_t dtype;                      /* ndlgpu_dtype */
+    int32_t rank;                       /* 1..NDLGPU_MAX_RANK */
+    int64_t extent[NDLGPU_MAX_RANK];
+    int64_t stride[NDLGPU_MAX_RANK];    /* elements, signed */
+} ndlgpu_view;
+
+/* One 1-D pass: taps[k] weighs the sample at offset k - center along `axis`
+ * (ndl centres kernels at K/2, image/detail.h:155-163; zero taps are
+ * skipped, image/detail.h:171-172).  taps is host memory. */
+typedef struct ndlgpu_axis_kernel {
+    int32_t axis;
+    int32_t ntaps;
+    int32_t center;
+    int32_t reserved;                   /* must be 0 */
+    const double* taps;
+} ndlgpu_axis_kernel;
+
+/* ---- library information ------------------------------------------------ */
+NDLGPU_API const char* ndlgpu_version(void);
+NDLGPU_API const char* ndlgpu_status_string(ndlgpu_status s);
+/* Detail of the last error returned on this host thread ("" if none). */
+NDLGPU_API const char* ndlgpu_last_error(void);
+
+/* ---- forward ------------------------------------------------------------ */
+
+/* ndl::convolve(src, dst, kernel, border)  -- processing/convolution.h:52-71.
+ * `kernel` is a HOST view of any dtype and the image's rank (each value is
+ * converted to double, convolution.h:68).  A kernel whose extent exceeds 1
+ * along one axis only is run by the separable kernels; any other kernel by
+ * the general N-D kernel.  Integral DstT truncates toward zero; arithmetic
+ * per ndlgpu_precision AUTO. */
+NDLGPU_API ndlgpu_status ndlgpu_convolve(const ndlgpu_view* src, const ndlgpu_view* dst,
+                              const ndlgpu_view* kernel, int border, void* stream);
+
+/* As ndlgpu_convolve with an explicit precision. */
+NDLGPU_API ndlgpu_status ndlgpu_convolve_ex(const ndlgpu_view* src, const ndlgpu_view* dst,
+                                 const ndlgpu_view* kernel, int border, int precision,
+                                 void* stream);
+
+/* ndl::gaussian_blur(src, dst, sigma, border) -- processing/convolution.h:107-186.
+ * Radius ceil(3*sigma) (mathHelpers.h:17-18), weights exp(-d^2/(2 sigma^2))
+ * normalised in double on the host (convolution.h:116-126), one pass per
+ * axis, one final rounding for integral DstT.  `workspace` may be NULL (the
+ * library then allocates stream-ordered scratch) or at least the size
+ * reported by ndlgpu_gaussian_blur_workspace_size(). */
+NDLGPU_API ndlgpu_status ndlgpu_gaussian_blur(const ndlgpu_view* src, const ndlgpu_view* dst,
+                                   double sigma, int border,
+                                   void* workspace, size_t workspace_bytes, void* stream);
+NDLGPU_API ndlgpu_status ndlgpu_gaussian_blur_workspace_size(const ndlgpu_view* src, const ndlgpu_view* dst,
+                                                  double sigma, int border, size_t* bytes);
+
+/* gaussian_blur() generalised to one sigma per axis (sigma[a] == 0 leaves
+ * axis a untouched).  Same weights, structure and rounding as
+ * ndlgpu_gaussian_blur; passes run in axis order. */
+NDLGPU_API ndlgpu_status ndlgpu_gaussian_blur_axes(const ndlgpu_view* src, const ndlgpu_view* dst,
+                                        const double* sigma_per_axis, int border,
+                                        void* workspace, size_t workspace_bytes, void* stream);
+
+/* A chain of 1-D passes (each a convolve() with a {1,..,K,..,1} kernel, the
+ * kernel gaussian_blur() builds at convolution.h:132-139) applied in order,
+ * composed per `compose` (ndlgpu_compose) with arithmetic per `precision`. */
+NDLGPU_API ndlgpu_status ndlgpu_convolve_axes(const ndlgpu_view* src, const ndlgpu_view* dst,
+                                   int npass, const ndlgpu_axis_kernel* passes,
+                                   int border, int compose, int precision,
+                                   void* workspace, size_t workspace_bytes, void* stream);
+NDLGPU_API ndlgpu_status ndlgpu_convolve_axes_workspace_size(const ndlgpu_view* src, const ndlgpu_view* dst,
+                                                  int npass, const ndlgpu_axis_kernel* passes,
+                                                  int border, int compose, int precision,
+                                                  size_t* bytes);
+
+/* ---- adjoint (no reference counterpart: the reference has no gradients) --
+ * For Y = P_n(...P_1(X)) (ROUND_ONCE composition, float types) and
+ * L = sum(grad_out * Y):
+ *   grad_src  (may be NULL)  <- dL/dX, the border-aware transpose: Clamp folds
+ *             out-of-range taps onto the edge samples, Reflect onto their
+ *             mirror images, Wrap onto the opposite end.
+ *   grad_taps (may be NULL)  <- dL/dw for every tap of every pass, back to
+ *             back in pass order (sum of ntaps values, dtype grad_taps_dtype
+ *             F32 or F64, device memory).  Needs `src` (the forward input).
+ * Deterministic: tap gradients are reduced in a fixed two-stage order. */
+NDLGPU_API ndlgpu_status ndlgpu_convolve_axes_adjoint(const ndlgpu_view* grad_out, const ndlgpu_view* src,
+                                           const ndlgpu_view* grad_src,
+                                           int npass, const ndlgpu_axis_kernel* passes, int border,
+                                           void* grad_taps, int grad_taps_dtype,
+                                           void* workspace, size_t workspace_bytes, void* stream);
+NDLGPU_API ndlgpu_status ndlgpu_convolve_axes_adjoint_workspace_size(const ndlgpu_view* grad_out, const ndlgpu_view* src,
+                                                          const ndlgpu_view* grad_src,
+                                                          int npass, const ndlgpu_axis_kernel* passes,
+                                                          int border, int grad_taps_dtype, size_t* bytes);
+
+/* ---- device guard word -------------------------------------------------- */
+/* Reads (and clears) the library's device-side guard word on the current
+ * device after synchronising `stream`: 0 if no kernel guard fired. */
+NDLGPU_API ndlgpu_status ndlgpu_device_status(void* stream, int32_t* code);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NDLGPU_H */

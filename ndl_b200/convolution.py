@@ -1,0 +1,169 @@
+"""Python mirror of ndl's convolution toolkit (processing/convolution.h),
+running on the B200 through the C ABI of libndlgpu.so.
+
+Same names, argument meaning and defaults as the reference:
+
+* ``convolve(src, dst, kernel, border=BorderMode.Clamp)``
+  -- processing/convolution.h:52-71
+* ``gaussian_blur(src, dst, sigma, border=BorderMode.Clamp)``
+  -- processing/convolution.h:107-186
+
+where ``src``/``dst`` are ``ndl_b200.Image`` views of device memory (any
+strides, including the negative ones ``mirror()`` makes) and ``kernel`` is a
+host array (numpy or nested list) in the same reversed axis order as
+``Image.tensor()`` (numpy dim 0 = ndl axis DIM-1).  The reference reports a
+wrong extent with assert(); here every precondition raises ``NdlGpuError``
+before any work is enqueued.  Calls are asynchronous on the current torch
+CUDA stream unless ``stream`` is given.
+
+Extensions beyond the reference (documented in include/ndlgpu.h):
+``gaussian_blur_axes`` (one sigma per axis), ``convolve_axes`` (a chain of
+1-D passes with explicit composition and precision) and
+``convolve_axes_adjoint`` (input and tap gradients).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import abi
+from .image import BorderMode, Image
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    if isinstance(stream, torch.cuda.Stream):
+        return ctypes.c_void_p(stream.cuda_stream)
+    return ctypes.c_void_p(int(stream))
+
+
+def _host_kernel_view(kernel, rank):
+    k = np.ascontiguousarray(np.asarray(kernel))
+    if k.dtype == np.bool_:
+        k = k.astype(np.uint8)
+    code = {np.dtype(np.uint8): abi.U8, np.dtype(np.int8): abi.I8, np.dtype(np.uint16): abi.U16,
+            np.dtype(np.int16): abi.I16, np.dtype(np.int32): abi.I32, np.dtype(np.uint32): abi.U32,
+            np.dtype(np.int64): abi.I64, np.dtype(np.uint64): abi.U64, np.dtype(np.float32): abi.F32,
+            np.dtype(np.float64): abi.F64, np.dtype(np.float16): abi.F16}.get(k.dtype)
+    if code is None:
+        k = k.astype(np.float64)
+        code = abi.F64
+    if k.ndim != rank:
+        raise ValueError("kernel rank %d != image rank %d" % (k.ndim, rank))
+    ext = list(k.shape[::-1])
+    st = [s // k.itemsize for s in k.strides[::-1]]
+    return abi.make_view(k.ctypes.data, code, ext, st), k
+
+
+def convolve(src: Image, dst: Image, kernel, border=BorderMode.Clamp, precision=abi.PREC_AUTO, stream=None):
+    """ndl::convolve(src, dst, kernel, border): correlation (kernel not
+    flipped), centred at K/2 per axis, zero taps skipped, border-mapped per
+    axis; integral DstT truncates (processing/convolution.h:52-71)."""
+    lib = abi.load()
+    kv, keep = _host_kernel_view(kernel, src.dim)
+    sv, dv = src.abi_view(), dst.abi_view()
+    abi.check(lib.ndlgpu_convolve_ex(ctypes.byref(sv), ctypes.byref(dv), ctypes.byref(kv), int(border),
+                                     int(precision), _stream_ptr(stream)))
+    del keep
+    return dst
+
+
+def gaussian_blur(src: Image, dst: Image, sigma: float, border=BorderMode.Clamp, workspace=None, stream=None):
+    """ndl::gaussian_blur(src, dst, sigma, border) (processing/convolution.h:107-186)."""
+    lib = abi.load()
+    sv, dv = src.abi_view(), dst.abi_view()
+    ws, wsb = _ws(workspace)
+    abi.check(lib.ndlgpu_gaussian_blur(ctypes.byref(sv), ctypes.byref(dv), ctypes.c_double(sigma), int(border),
+                                       ws, wsb, _stream_ptr(stream)))
+    return dst
+
+
+def gaussian_blur_axes(src: Image, dst: Image, sigmas, border=BorderMode.Clamp, workspace=None, stream=None):
+    """gaussian_blur with one sigma per axis (0 leaves an axis untouched)."""
+    lib = abi.load()
+    sig = (ctypes.c_double * src.dim)(*[float(s) for s in sigmas])
+    sv, dv = src.abi_view(), dst.abi_view()
+    ws, wsb = _ws(workspace)
+    abi.check(lib.ndlgpu_gaussian_blur_axes(ctypes.byref(sv), ctypes.byref(dv), sig, int(border), ws, wsb,
+                                            _stream_ptr(stream)))
+    return dst
+
+
+def convolve_axes(src: Image, dst: Image, passes, border=BorderMode.Clamp, compose=abi.ROUND_ONCE,
+                  precision=abi.PREC_AUTO, workspace=None, stream=None):
+    """A chain of 1-D passes [(axis, taps[, center]), ...] applied in order."""
+    lib = abi.load()
+    arr, keep = abi.make_passes(passes)
+    sv, dv = src.abi_view(), dst.abi_view()
+    ws, wsb = _ws(workspace)
+    abi.check(lib.ndlgpu_convolve_axes(ctypes.byref(sv), ctypes.byref(dv), len(arr), arr, int(border),
+                                       int(compose), int(precision), ws, wsb, _stream_ptr(stream)))
+    del keep
+    return dst
+
+
+def convolve_axes_workspace_size(src: Image, dst: Image, passes, border=BorderMode.Clamp, compose=abi.ROUND_ONCE,
+                                 precision=abi.PREC_AUTO):
+    lib = abi.load()
+    arr, keep = abi.make_passes(passes)
+    sv, dv = src.abi_view(), dst.abi_view()
+    n = ctypes.c_size_t(0)
+    abi.check(lib.ndlgpu_convolve_axes_workspace_size(ctypes.byref(sv), ctypes.byref(dv), len(arr), arr, int(border),
+                                                      int(compose), int(precision), ctypes.byref(n)))
+    del keep
+    return n.value
+
+
+def convolve_axes_adjoint(grad_out: Image, src, grad_src, passes, border=BorderMode.Clamp, grad_taps=None,
+                          workspace=None, stream=None):
+    """Gradients of L = sum(grad_out * Y), Y = the ROUND_ONCE chain of
+    ``passes`` applied to ``src``: writes dL/dsrc into ``grad_src`` (an Image,
+    or None) and dL/dtaps into ``grad_taps`` (a 1-D float32/float64 CUDA
+    tensor of sum(ntaps) values, or None; needs ``src``)."""
+    lib = abi.load()
+    arr, keep = abi.make_passes(passes)
+    gv = grad_out.abi_view()
+    sv = src.abi_view() if src is not None else None
+    xv = grad_src.abi_view() if grad_src is not None else None
+    tp, tdt = None, abi.F32
+    if grad_taps is not None:
+        if not (grad_taps.is_cuda and grad_taps.is_contiguous() and grad_taps.dtype in (torch.float32, torch.float64)):
+            raise ValueError("grad_taps must be a contiguous float32/float64 CUDA tensor")
+        tp = ctypes.c_void_p(grad_taps.data_ptr())
+        tdt = abi.F32 if grad_taps.dtype == torch.float32 else abi.F64
+    ws, wsb = _ws(workspace)
+    abi.check(lib.ndlgpu_convolve_axes_adjoint(ctypes.byref(gv), ctypes.byref(sv) if sv else None,
+                                               ctypes.byref(xv) if xv else None, len(arr), arr, int(border),
+                                               tp, tdt, ws, wsb, _stream_ptr(stream)))
+    del keep
+    return grad_src, grad_taps
+
+
+def _ws(workspace):
+    if workspace is None:
+        return None, 0
+    if isinstance(workspace, torch.Tensor):
+        return ctypes.c_void_p(workspace.data_ptr()), workspace.numel() * workspace.element_size()
+    ptr, nbytes = workspace
+    return ctypes.c_void_p(int(ptr)), int(nbytes)
+
+
+def gaussian_radius(sigma: float) -> int:
+    """_kernelSize(sigma) = _ceil(3.0f * sigma) (mathHelpers.h:17-18)."""
+    num = 3.0 * float(sigma)
+    t = int(num)
+    return t if float(t) == num else t + (1 if num > 0 else 0)
+
+
+def gaussian_taps(sigma: float) -> np.ndarray:
+    """The normalised taps gaussian_blur builds (processing/convolution.h:116-126)."""
+    r = gaussian_radius(sigma)
+    d = np.arange(-r, r + 1, dtype=np.float64)
+    w = np.exp(-(d * d) / (2 * sigma * sigma))
+    s = 0.0
+    for x in w:          # summed in index order like the reference
+        s += float(x)
+    return w / s

@@ -1,0 +1,1167 @@
+// host.cpp -- the C ABI (include/ndlgpu.h): validation, view canonicalisation,
+// planning and launch.  Host-only C++17.
+//
+// Every entry point validates its arguments completely before the first CUDA
+// call, so an error return means nothing was enqueued (the reference checks
+// with assert() only, processing/convolution.h:59,112 and image/core.h:557).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+
+namespace ndlgpu {
+
+static thread_local std::string t_last_error;
+
+static ndlgpu_status fail(ndlgpu_status s, const std::string& msg)
+{
+    t_last_error = msg;
+    return s;
+}
+
+static ndlgpu_status cuda_fail(cudaError_t e, const char* what)
+{
+    if (e == cudaErrorMemoryAllocation) return fail(NDLGPU_ERR_OUT_OF_MEMORY, std::string(what) + ": out of device memory");
+    return fail(NDLGPU_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// ---------------------------------------------------------------------------
+// Views
+// ---------------------------------------------------------------------------
+
+static ndlgpu_status check_view(const ndlgpu_view* v, const char* name, bool device_data)
+{
+    if (!v) return fail(NDLGPU_ERR_INVALID_ARGUMENT, std::string(name) + " is NULL");
+    if (v->rank < 1 || v->rank > kMaxRank)
+        return fail(NDLGPU_ERR_INVALID_ARGUMENT, std::string(name) + ": rank must be 1..8");
+    if (!dtype_valid(v->dtype)) return fail(NDLGPU_ERR_UNSUPPORTED_DTYPE, std::string(name) + ": unknown dtype");
+    __int128 span = 0;
+    bool empty = false;
+    for (int i = 0; i < v->rank; i++) {
+        if (v->extent[i] < 0) return fail(NDLGPU_ERR_INVALID_ARGUMENT, std::string(name) + ": negative extent");
+        if (v->extent[i] == 0) empty = true;
+        if (v->extent[i] > 0x7fffffffLL)
+            return fail(NDLGPU_ERR_INDEX_OVERFLOW, std::string(name) + ": extent exceeds 2^31-1");
+        const __int128 s = v->stride[i] < 0 ? -(__int128)v->stride[i] : (__int128)v->stride[i];
+        span += s * (__int128)(v->extent[i] > 0 ? v->extent[i] - 1 : 0);
+    }
+    if (span > ((__int128)1 << 62)) return fail(NDLGPU_ERR_INDEX_OVERFLOW, std::string(name) + ": view spans more than 2^62 elements");
+    if (!empty && device_data && !v->data) return fail(NDLGPU_ERR_INVALID_ARGUMENT, std::string(name) + ": data is NULL");
+    return NDLGPU_OK;
+}
+
+static int64_t view_count(const ndlgpu_view* v)
+{
+    int64_t n = 1;
+    for (int i = 0; i < v->rank; i++) n *= v->extent[i];
+    return n;
+}
+
+// Byte range [lo, hi) covered by a view.
+static void view_bytes(const ndlgpu_view* v, intptr_t* lo, intptr_t* hi)
+{
+    const int es = dtype_size(v->dtype);
+    int64_t mn = 0, mx = 0;
+    for (int i = 0; i < v->rank; i++) {
+        const int64_t d = v->stride[i] * (v->extent[i] - 1);
+        if (d < 0) mn += d; else mx += d;
+    }
+    *lo = (intptr_t)v->data + (intptr_t)mn * es;
+    *hi = (intptr_t)v->data + (intptr_t)mx * es + es;
+}
+
+static ndlgpu_status check_pair(const ndlgpu_view* src, const ndlgpu_view* dst)
+{
+    if (src->rank != dst->rank) return fail(NDLGPU_ERR_EXTENT_MISMATCH, "src and dst ranks differ");
+    for (int i = 0; i < src->rank; i++)
+        if (src->extent[i] != dst->extent[i])
+            return fail(NDLGPU_ERR_EXTENT_MISMATCH, "dst.extent() != src.extent() (convolution.h:59) on axis " + std::to_string(i));
+    if (view_count(src) == 0) return NDLGPU_OK;
+    intptr_t a0, a1, b0, b1;
+    view_bytes(src, &a0, &a1);
+    view_bytes(dst, &b0, &b1);
+    if (a0 < b1 && b0 < a1) return fail(NDLGPU_ERR_ALIASING, "src and dst memory overlap (in-place convolution is not supported)");
+    // dst must not write one address twice: with axes sorted by |stride|,
+    // each axis must step over everything the faster axes cover.
+    std::vector<std::pair<int64_t, int64_t>> ax;
+    for (int i = 0; i < dst->rank; i++)
+        if (dst->extent[i] > 1) ax.push_back({dst->stride[i] < 0 ? -dst->stride[i] : dst->stride[i], dst->extent[i]});
+    std::sort(ax.begin(), ax.end());
+    int64_t covered = 1;
+    for (auto& a : ax) {
+        if (a.first < covered) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "dst view overlaps itself (a stride is smaller than the span of the faster axes)");
+        covered = a.first * a.second;
+    }
+    return NDLGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Canonical problem
+// ---------------------------------------------------------------------------
+
+struct CAxis {
+    int64_t n, ss, ds;
+    int logical;
+};
+
+struct CPass {
+    int axis;                 // canonical axis index
+    std::vector<int> off;     // nonzero taps, summation order
+    std::vector<double> w;
+};
+
+struct Canon {
+    const char* src;
+    char* dst;
+    int sdt, ddt;
+    std::vector<CAxis> ax;
+    std::vector<CPass> passes;
+    int64_t total;
+};
+
+// Input pass description (logical axis).
+struct LPass {
+    int axis;
+    int center;
+    std::vector<double> taps;
+};
+
+static ndlgpu_status canonicalise(const ndlgpu_view* src, const ndlgpu_view* dst,
+                                  const std::vector<LPass>& lp, int border, Canon* out)
+{
+    const int R = src->rank;
+    if (border < NDLGPU_CLAMP || border > NDLGPU_REFLECT) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "unknown border mode");
+    Canon c;
+    c.src = (const char*)src->data;
+    c.dst = (char*)dst->data;
+    c.sdt = src->dtype;
+    c.ddt = dst->dtype;
+    c.total = view_count(src);
+    const int ses = dtype_size(c.sdt), des = dtype_size(c.ddt);
+
+    // passes, with the one-period rule for Wrap/Reflect (mathHelpers.h:23-24
+    // wrap/reflect once; a larger offset would index outside the image)
+    std::vector<CPass> passes;
+    for (const LPass& p : lp) {
+        if (p.axis < 0 || p.axis >= R) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "pass axis out of range");
+        if (p.taps.empty()) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "a pass has no taps");
+        if ((int)p.taps.size() > kMaxTaps) return fail(NDLGPU_ERR_TOO_MANY_TAPS, "a pass has more than 255 taps");
+        CPass cp;
+        cp.axis = p.axis;
+        for (int k = 0; k < (int)p.taps.size(); k++) {
+            if (p.taps[k] == 0.0) continue;   // image/detail.h:171-172
+            const int o = k - p.center;
+            if (border != NDLGPU_CLAMP && c.total > 0 && (o > src->extent[p.axis] || o < -src->extent[p.axis]))
+                return fail(NDLGPU_ERR_RADIUS_EXCEEDS_EXTENT,
+                            "tap offset " + std::to_string(o) + " exceeds the extent " + std::to_string(src->extent[p.axis]) +
+                                " of axis " + std::to_string(p.axis) + " (Wrap/Reflect map one period only)");
+            cp.off.push_back(o);
+            cp.w.push_back(p.taps[k]);
+        }
+        passes.push_back(cp);
+    }
+    if (c.total == 0) {
+        *out = c;
+        return NDLGPU_OK;
+    }
+
+    // flip negative source strides (the border maps are symmetric under
+    // reversal, so only the tap offsets change sign; summation order kept)
+    std::vector<CAxis> ax(R);
+    std::vector<bool> has_pass(R, false);
+    for (auto& p : passes) has_pass[p.axis] = true;
+    for (int i = 0; i < R; i++) {
+        CAxis a{src->extent[i], src->stride[i], dst->stride[i], i};
+        if (a.ss < 0) {
+            c.src += (intptr_t)(a.n - 1) * a.ss * ses;
+            c.dst += (intptr_t)(a.n - 1) * a.ds * des;
+            a.ss = -a.ss;
+            a.ds = -a.ds;
+            for (auto& p : passes)
+                if (p.axis == i)
+                    for (auto& o : p.off) o = -o;
+        }
+        ax[i] = a;
+    }
+    // drop extent-1 axes without passes; order by source stride
+    std::vector<int> keep;
+    for (int i = 0; i < R; i++)
+        if (ax[i].n > 1 || has_pass[i]) keep.push_back(i);
+    if (keep.empty()) keep.push_back(0);
+    std::stable_sort(keep.begin(), keep.end(), [&](int a, int b) { return ax[a].ss < ax[b].ss; });
+    std::vector<int> pos(R, -1);
+    for (int k = 0; k < (int)keep.size(); k++) {
+        c.ax.push_back(ax[keep[k]]);
+        pos[keep[k]] = k;
+    }
+    for (auto& p : passes) p.axis = pos[p.axis];
+    c.passes = passes;
+    *out = c;
+    return NDLGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Arithmetic selection
+// ---------------------------------------------------------------------------
+
+static double max_abs_of(int dt)
+{
+    switch (dt) {
+    case NDLGPU_U8: return 255;
+    case NDLGPU_I8: return 128;
+    case NDLGPU_U16: return 65535;
+    case NDLGPU_I16: return 32768;
+    default: return -1;   // not eligible for the int32 path
+    }
+}
+
+// Smallest shift s <= 20 with every weight an integer multiple of 2^-s and
+// |numerator| < 2^20; -1 if none (the taps are not all dyadic).
+static int dyadic_shift(const std::vector<double>& w, std::vector<int32_t>* num)
+{
+    for (int s = 0; s <= 20; s++) {
+        bool ok = true;
+        const double scale = std::ldexp(1.0, s);
+        for (double x : w) {
+            const double y = x * scale;   // exact (power-of-two scale)
+            if (!(std::fabs(y) < 1048576.0) || y != std::floor(y)) { ok = false; break; }
+        }
+        if (ok) {
+            if (num) {
+                num->clear();
+                for (double x : w) num->push_back((int32_t)(x * scale));
+            }
+            return s;
+        }
+    }
+    return -1;
+}
+
+// Integer path eligibility: integral src and dst, all taps dyadic and every
+// partial sum bounded by 2^31 (so the reference's double sums are exact too).
+static bool int_path_ok(const Canon& c, int compose)
+{
+    if (!dtype_integral(c.ddt)) return false;
+    double in_max = max_abs_of(c.sdt);
+    if (in_max < 0) return false;
+    if (compose == NDLGPU_CAST_EACH && c.passes.size() > 1 && max_abs_of(c.ddt) < 0) return false;
+    double bound = in_max;
+    int shift = 0;
+    for (size_t i = 0; i < c.passes.size(); i++) {
+        std::vector<int32_t> m;
+        const int s = dyadic_shift(c.passes[i].w, &m);
+        if (s < 0) return false;
+        double sum = 0;
+        for (int32_t v : m) sum += std::fabs((double)v);
+        if (compose == NDLGPU_CAST_EACH) {
+            const double b = (i == 0 ? in_max : max_abs_of(c.ddt)) * sum;
+            if (!(b < 2147483647.0)) return false;
+        } else {
+            bound *= sum;
+            shift += s;
+        }
+    }
+    if (compose != NDLGPU_CAST_EACH && !(bound < 2147483647.0 && shift <= 30)) return false;
+    return true;
+}
+
+static Acc pick_acc(const Canon& c, int compose, int precision)
+{
+    const bool intok = int_path_ok(c, compose);
+    if (precision == NDLGPU_PREC_EXACT) return intok ? Acc::I32 : Acc::F64;
+    if (precision == NDLGPU_PREC_FP32) return Acc::F32;
+    if (dtype_integral(c.ddt)) return intok ? Acc::I32 : Acc::F64;
+    if (c.ddt == NDLGPU_F64 || c.sdt == NDLGPU_F64) return Acc::F64;
+    return Acc::F32;
+}
+
+// ---------------------------------------------------------------------------
+// Workspace
+// ---------------------------------------------------------------------------
+
+struct Scratch {
+    void* base = nullptr;
+    bool owned = false;
+    cudaStream_t stream = nullptr;
+    ~Scratch()
+    {
+        if (owned && base) cudaFreeAsync(base, stream);
+    }
+};
+
+static size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
+
+static ndlgpu_status get_scratch(size_t need, void* ws, size_t ws_bytes, cudaStream_t s, Scratch* sc)
+{
+    if (need == 0) return NDLGPU_OK;
+    if (ws) {
+        if (ws_bytes < need)
+            return fail(NDLGPU_ERR_WORKSPACE, "workspace of " + std::to_string(ws_bytes) + " bytes is smaller than the " +
+                                                  std::to_string(need) + " bytes required");
+        sc->base = ws;
+        return NDLGPU_OK;
+    }
+    cudaError_t e = cudaMallocAsync(&sc->base, need, s);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMallocAsync(workspace)");
+    sc->owned = true;
+    sc->stream = s;
+    return NDLGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Generic pass chain
+// ---------------------------------------------------------------------------
+
+static void fill_div(GenericPassParams& p)
+{
+    for (int i = 0; i < p.rank; i++) p.div[i].init((uint32_t)p.n[i]);
+}
+
+// One pass between two canonical buffers (strides given per canonical axis),
+// split into launches of < 2^31 outputs along the slowest non-pass axis.
+static ndlgpu_status run_generic_pass(Acc acc, const Canon& c, const CPass& pass,
+                                      const char* in, int in_dt, const std::vector<int64_t>& in_st,
+                                      char* out, int out_dt, const std::vector<int64_t>& out_st,
+                                      int border, int store_mode, int shift, const std::vector<int32_t>& num,
+                                      cudaStream_t s, bool transpose = false)
+{
+    const int R = (int)c.ax.size();
+    GenericPassParams p;
+    std::memset(&p, 0, sizeof(p));
+    p.src_dtype = in_dt;
+    p.dst_dtype = out_dt;
+    p.rank = R;
+    p.axis = pass.axis;
+    p.ntap = (int)pass.off.size();
+    p.border = border;
+    p.store_mode = store_mode;
+    p.shift = shift;
+    for (int t = 0; t < p.ntap; t++) {
+        p.off[t] = pass.off[t];
+        p.wd[t] = pass.w[t];
+        p.wf[t] = (float)pass.w[t];
+        p.wi[t] = num.empty() ? 0 : num[t];
+    }
+    for (int i = 0; i < R; i++) {
+        p.n[i] = c.ax[i].n;
+        p.ss[i] = in_st[i];
+        p.ds[i] = out_st[i];
+    }
+    // chunking axis: slowest axis that is not the pass axis
+    int cax = -1;
+    for (int i = R - 1; i >= 0; i--)
+        if (i != pass.axis) { cax = i; break; }
+    int64_t per = c.total;
+    int64_t chunk_n = 1;
+    if (c.total >= (int64_t(1) << 31)) {
+        if (cax < 0) return fail(NDLGPU_ERR_INDEX_OVERFLOW, "a single 1-D pass of 2^31 or more elements is not supported");
+        per = c.total / c.ax[cax].n;
+        chunk_n = std::max<int64_t>(1, ((int64_t(1) << 31) - 1) / per);
+        if (per >= (int64_t(1) << 31)) return fail(NDLGPU_ERR_INDEX_OVERFLOW, "view too large for the general kernel");
+    }
+    const int ies = dtype_size(in_dt), oes = dtype_size(out_dt);
+    if (chunk_n == 1 && c.total < (int64_t(1) << 31)) {
+        p.src = in;
+        p.dst = out;
+        p.total = (uint32_t)c.total;
+        fill_div(p);
+        cudaError_t e = transpose ? launch_pass_adjoint(acc, p, s) : launch_generic_pass(acc, p, s);
+        if (e != cudaSuccess) return cuda_fail(e, "generic pass");
+        return NDLGPU_OK;
+    }
+    for (int64_t b = 0; b < c.ax[cax].n; b += chunk_n) {
+        const int64_t m = std::min<int64_t>(chunk_n, c.ax[cax].n - b);
+        p.n[cax] = m;
+        p.src = in + (intptr_t)b * in_st[cax] * ies;
+        p.dst = out + (intptr_t)b * out_st[cax] * oes;
+        p.total = (uint32_t)(per * m);
+        fill_div(p);
+        if (transpose) return fail(NDLGPU_ERR_INDEX_OVERFLOW, "adjoint views of 2^31 or more elements are not supported");
+        cudaError_t e = launch_generic_pass(acc, p, s);
+        if (e != cudaSuccess) return cuda_fail(e, "generic pass");
+    }
+    return NDLGPU_OK;
+}
+
+static std::vector<int64_t> contiguous_strides(const Canon& c)
+{
+    std::vector<int64_t> st(c.ax.size());
+    int64_t m = 1;
+    for (size_t i = 0; i < c.ax.size(); i++) {
+        st[i] = m;
+        m *= c.ax[i].n;
+    }
+    return st;
+}
+
+struct Plan {
+    Acc acc;
+    bool fused = false;
+    FusedParams fp;
+    int nscratch = 0;       // intermediate buffers for the generic chain
+    int scratch_dtype = 0;
+};
+
+// Fused-kernel eligibility and parameters.
+static bool plan_fused(const Canon& c, Acc acc, int compose, int border, FusedParams* fp)
+{
+    if (acc != Acc::F32 && acc != Acc::I32) return false;
+    if (c.passes.empty() || c.passes.size() > 3) return false;
+    if (compose == NDLGPU_CAST_EACH && c.passes.size() > 1) {
+        // per-pass DstT rounding is the identity only for f32 results
+        if (!(acc == Acc::F32 && c.ddt == NDLGPU_F32)) return false;
+    }
+    const int R = (int)c.ax.size();
+    int kx = 1, ky = 1, kz = 1;
+    int role[3] = {0, -1, -1};   // canonical axis of X, Y, Z
+    std::vector<bool> used(R, false);
+    used[0] = true;
+    std::vector<const CPass*> by_axis(R, nullptr);
+    for (auto& p : c.passes) {
+        if (by_axis[p.axis]) return false;   // two passes on one axis
+        by_axis[p.axis] = &p;
+    }
+    // tap lists must be dense, odd and centred (offsets -K/2 .. K/2) in
+    // either direction; the order does not matter for F32/I32 sums
+    auto dense = [&](const CPass* p, int* K) {
+        if (!p) { *K = 1; return true; }
+        std::vector<int> o = p->off;
+        std::sort(o.begin(), o.end());
+        const int k = (int)o.size();
+        if (k % 2 == 0 || k > 37) return false;
+        for (int i = 0; i < k; i++)
+            if (o[i] != i - k / 2) return false;
+        *K = k;
+        return true;
+    };
+    std::vector<int> others;
+    for (int i = 1; i < R; i++)
+        if (by_axis[i]) others.push_back(i);
+    if (others.size() > 2) return false;
+    for (int i = 1; i < R && others.size() < 2; i++)
+        if (!by_axis[i] && std::find(others.begin(), others.end(), i) == others.end()) others.push_back(i);
+    std::sort(others.begin(), others.end());
+    if (others.size() >= 1) role[1] = others[0];
+    if (others.size() >= 2) role[2] = others[1];
+    for (int r = 0; r < 3; r++)
+        if (role[r] >= 0) used[role[r]] = true;
+    if (!dense(by_axis[0], &kx)) return false;
+    if (role[1] >= 0 && !dense(by_axis[role[1]], &ky)) return false;
+    if (role[2] >= 0 && !dense(by_axis[role[2]], &kz)) return false;
+    if (!fused_supported(acc, c.sdt, c.ddt, kx, ky, kz)) return false;
+
+    FusedParams& p = *fp;
+    std::memset(&p, 0, sizeof(p));
+    p.src = c.src;
+    p.dst = c.dst;
+    p.src_dtype = c.sdt;
+    p.dst_dtype = c.ddt;
+    p.border = border;
+    p.store_mode = (dtype_integral(c.ddt) && c.passes.size() > 1 && compose == NDLGPU_ROUND_ONCE) ? STORE_ROUND : STORE_CAST;
+    auto geo = [&](int r, int* n, int64_t* s, int64_t* d) {
+        if (role[r] < 0) { *n = 1; *s = 0; *d = 0; return; }
+        *n = (int)c.ax[role[r]].n;
+        *s = c.ax[role[r]].ss;
+        *d = c.ax[role[r]].ds;
+    };
+    geo(0, &p.nx, &p.sx, &p.dx);
+    geo(1, &p.ny, &p.sy, &p.dy);
+    geo(2, &p.nz, &p.sz, &p.dz);
+    // remaining axes must merge into one affine batch axis
+    int64_t nb = 1, sb = 0, db = 0;
+    for (int i = 0; i < R; i++) {
+        if (used[i]) continue;
+        if (nb == 1) { nb = c.ax[i].n; sb = c.ax[i].ss; db = c.ax[i].ds; continue; }
+        if (c.ax[i].ss != sb * nb || c.ax[i].ds != db * nb) return false;
+        nb *= c.ax[i].n;
+    }
+    if (nb > 0x7fffffffLL) return false;
+    p.nbatch = (int)nb;
+    p.sb = sb;
+    p.db = db;
+    p.kx = kx; p.ky = ky; p.kz = kz;
+    p.cx = kx / 2; p.cy = ky / 2; p.cz = kz / 2;
+    // weights in ascending offset order
+    auto fill = [&](const CPass* cp, int K, float* wf, int32_t* wi, int* shift) {
+        if (!cp) { wf[0] = 1.0f; wi[0] = 1; return; }
+        std::vector<std::pair<int, double>> t;
+        for (size_t i = 0; i < cp->off.size(); i++) t.push_back({cp->off[i], cp->w[i]});
+        std::sort(t.begin(), t.end());
+        std::vector<double> w;
+        for (auto& x : t) w.push_back(x.second);
+        for (int k = 0; k < K; k++) wf[k] = (float)w[k];
+        if (acc == Acc::I32) {
+            std::vector<int32_t> m;
+            *shift += dyadic_shift(w, &m);
+            for (int k = 0; k < K; k++) wi[k] = m[k];
+        }
+    };
+    int shift = 0;
+    fill(by_axis[0], kx, p.wxf, p.wxi, &shift);
+    fill(role[1] >= 0 ? by_axis[role[1]] : nullptr, ky, p.wyf, p.wyi, &shift);
+    fill(role[2] >= 0 ? by_axis[role[2]] : nullptr, kz, p.wzf, p.wzi, &shift);
+    p.shift = shift;
+    // Z chunk: enough CTAs for two waves over the SMs, chunks >= 4*KZ planes
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long long tiles = (long long)((p.nx + 63) / 64) * ((p.ny + 31) / 32) * p.nbatch;
+    int chunks = (int)std::min<long long>(std::max<long long>(1, (2LL * sms + tiles - 1) / tiles), 65535);
+    int zc = (p.nz + chunks - 1) / chunks;
+    zc = std::max(zc, std::min(p.nz, 4 * kz));
+    p.zchunk = std::max(1, zc);
+    return true;
+}
+
+static ndlgpu_status plan(const Canon& c, int compose, int precision, int border, Plan* pl)
+{
+    pl->acc = pick_acc(c, compose, precision);
+    pl->fused = plan_fused(c, pl->acc, compose, border, &pl->fp);
+    if (pl->fused || c.passes.size() <= 1) {
+        pl->nscratch = 0;
+        return NDLGPU_OK;
+    }
+    pl->nscratch = c.passes.size() == 2 ? 1 : 2;
+    if (compose == NDLGPU_CAST_EACH) pl->scratch_dtype = c.ddt;
+    else pl->scratch_dtype = acc_dtype(pl->acc);
+    return NDLGPU_OK;
+}
+
+static size_t plan_workspace(const Canon& c, const Plan& pl)
+{
+    if (pl.nscratch == 0) return 0;
+    return (size_t)pl.nscratch * align_up((size_t)c.total * dtype_size(pl.scratch_dtype));
+}
+
+static ndlgpu_status execute(const Canon& c, const Plan& pl, int compose, int border, void* ws, size_t ws_bytes,
+                             cudaStream_t s)
+{
+    if (c.total == 0) return NDLGPU_OK;
+    if (pl.fused) {
+        cudaError_t e = launch_fused(pl.acc, pl.fp, s);
+        if (e != cudaSuccess) return cuda_fail(e, "fused kernel");
+        return NDLGPU_OK;
+    }
+    const int R = (int)c.ax.size();
+    std::vector<int64_t> sst(R), dst_st(R);
+    for (int i = 0; i < R; i++) {
+        sst[i] = c.ax[i].ss;
+        dst_st[i] = c.ax[i].ds;
+    }
+    const size_t need = plan_workspace(c, pl);
+    Scratch sc;
+    ndlgpu_status st = get_scratch(need, ws, ws_bytes, s, &sc);
+    if (st != NDLGPU_OK) return st;
+    char* buf[2] = {nullptr, nullptr};
+    if (pl.nscratch >= 1) buf[0] = (char*)sc.base;
+    if (pl.nscratch >= 2) buf[1] = (char*)sc.base + align_up((size_t)c.total * dtype_size(pl.scratch_dtype));
+    const std::vector<int64_t> cst = contiguous_strides(c);
+
+    const int np = (int)c.passes.size();
+    if (np == 0) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "no passes");
+    const bool integral_dst = dtype_integral(c.ddt);
+    const char* in = c.src;
+    int in_dt = c.sdt;
+    std::vector<int64_t> in_st = sst;
+    for (int p = 0; p < np; p++) {
+        const bool last = (p == np - 1);
+        char* out = last ? c.dst : buf[p % 2];
+        const int out_dt = last ? c.ddt : pl.scratch_dtype;
+        const std::vector<int64_t>& out_st = last ? dst_st : cst;
+        int mode;
+        int shift = 0;
+        std::vector<int32_t> num;
+        if (pl.acc == Acc::I32) {
+            shift = dyadic_shift(c.passes[p].w, &num);
+        }
+        if (compose == NDLGPU_CAST_EACH || np == 1) {
+            mode = STORE_CAST;
+        } else if (!last) {
+            mode = (pl.acc == Acc::I32) ? STORE_RAW : STORE_CAST;
+        } else {
+            mode = integral_dst ? STORE_ROUND : STORE_CAST;
+        }
+        if (pl.acc == Acc::I32 && compose != NDLGPU_CAST_EACH && np > 1) {
+            // raw integer sums carry the scale until the last pass
+            if (!last) shift = 0;
+            else {
+                shift = 0;
+                for (int q = 0; q < np; q++) shift += dyadic_shift(c.passes[q].w, nullptr);
+            }
+        }
+        ndlgpu_status r = run_generic_pass(pl.acc, c, c.passes[p], in, in_dt, in_st, out, out_dt, out_st, border,
+                                           mode, shift, num, s);
+        if (r != NDLGPU_OK) return r;
+        in = out;
+        in_dt = out_dt;
+        in_st = out_st;
+    }
+    return NDLGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Gaussian weights: processing/convolution.h:116-126 with the radius rule
+// _kernelSize(sigma) = _ceil(3.0f * sigma) of mathHelpers.h:17-18.
+// ---------------------------------------------------------------------------
+
+static int kernel_size(double sigma)
+{
+    const double num = 3.0f * sigma;
+    const int t = static_cast<int>(num);
+    return (static_cast<double>(t) == num) ? t : t + ((num > 0) ? 1 : 0);
+}
+
+static std::vector<double> gaussian_taps(double sigma)
+{
+    const int radius = kernel_size(sigma);
+    const int width = 2 * radius + 1;
+    std::vector<double> w((size_t)width);
+    double wsum = 0;
+    for (int i = 0; i < width; i++) {
+        const double d = i - radius;
+        w[i] = std::exp(-(d * d) / (2 * sigma * sigma));
+        wsum += w[i];
+    }
+    for (auto& x : w) x /= wsum;
+    return w;
+}
+
+// ---------------------------------------------------------------------------
+// Shared front end of the pass-chain entry points
+// ---------------------------------------------------------------------------
+
+static ndlgpu_status prepare(const ndlgpu_view* src, const ndlgpu_view* dst, const std::vector<LPass>& lp,
+                             int border, int compose, int precision, Canon* c, Plan* pl)
+{
+    ndlgpu_status st;
+    if ((st = check_view(src, "src", true)) != NDLGPU_OK) return st;
+    if ((st = check_view(dst, "dst", true)) != NDLGPU_OK) return st;
+    if ((st = check_pair(src, dst)) != NDLGPU_OK) return st;
+    if (compose != NDLGPU_ROUND_ONCE && compose != NDLGPU_CAST_EACH)
+        return fail(NDLGPU_ERR_INVALID_ARGUMENT, "unknown compose mode");
+    if (precision < NDLGPU_PREC_AUTO || precision > NDLGPU_PREC_EXACT)
+        return fail(NDLGPU_ERR_INVALID_ARGUMENT, "unknown precision");
+    if (lp.empty()) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "at least one pass is required");
+    if ((st = canonicalise(src, dst, lp, border, c)) != NDLGPU_OK) return st;
+    if (c->total == 0) return NDLGPU_OK;
+    return plan(*c, compose, precision, border, pl);
+}
+
+static ndlgpu_status lpasses_from(int npass, const ndlgpu_axis_kernel* passes, std::vector<LPass>* out)
+{
+    if (npass < 1 || !passes) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "npass must be >= 1 and passes non-NULL");
+    for (int i = 0; i < npass; i++) {
+        const ndlgpu_axis_kernel& k = passes[i];
+        if (k.ntaps < 1 || !k.taps) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "a pass has no taps");
+        if (k.ntaps > kMaxTaps) return fail(NDLGPU_ERR_TOO_MANY_TAPS, "a pass has more than 255 taps");
+        if (k.reserved != 0) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "ndlgpu_axis_kernel.reserved must be 0");
+        LPass lp;
+        lp.axis = k.axis;
+        lp.center = k.center;
+        lp.taps.assign(k.taps, k.taps + k.ntaps);
+        out->push_back(lp);
+    }
+    return NDLGPU_OK;
+}
+
+static ndlgpu_status gaussian_passes(const ndlgpu_view* src, const double* sigma, bool per_axis,
+                                     std::vector<LPass>* out)
+{
+    if (!src || src->rank < 1 || src->rank > kMaxRank) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "bad src view");
+    for (int a = 0; a < src->rank; a++) {
+        const double s = per_axis ? sigma[a] : sigma[0];
+        if (per_axis && s == 0.0) continue;
+        if (!(s > 0) || !std::isfinite(s)) return fail(NDLGPU_ERR_BAD_SIGMA, "sigma must be positive and finite (convolution.h:112)");
+        LPass lp;
+        lp.axis = a;
+        lp.taps = gaussian_taps(s);
+        lp.center = (int)lp.taps.size() / 2;
+        if ((int)lp.taps.size() > kMaxTaps) return fail(NDLGPU_ERR_TOO_MANY_TAPS, "sigma too large (more than 255 taps)");
+        out->push_back(lp);
+    }
+    if (out->empty()) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "every sigma is zero");
+    return NDLGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Host reading of a kernel view (ndlgpu_convolve's kernel is host memory)
+// ---------------------------------------------------------------------------
+
+static double host_value(const ndlgpu_view* k, int64_t off)
+{
+    const char* b = (const char*)k->data;
+    switch (k->dtype) {
+    case NDLGPU_U8: return ((const uint8_t*)b)[off];
+    case NDLGPU_I8: return ((const int8_t*)b)[off];
+    case NDLGPU_U16: return ((const uint16_t*)b)[off];
+    case NDLGPU_I16: return ((const int16_t*)b)[off];
+    case NDLGPU_I32: return ((const int32_t*)b)[off];
+    case NDLGPU_U32: return ((const uint32_t*)b)[off];
+    case NDLGPU_I64: return (double)((const int64_t*)b)[off];
+    case NDLGPU_U64: return (double)((const uint64_t*)b)[off];
+    case NDLGPU_F32: return ((const float*)b)[off];
+    case NDLGPU_F64: return ((const double*)b)[off];
+    case NDLGPU_F16: {
+        uint16_t h = ((const uint16_t*)b)[off];
+        const int e = (h >> 10) & 31, m = h & 1023;
+        const double sgn = (h & 0x8000) ? -1.0 : 1.0;
+        if (e == 0) return sgn * std::ldexp((double)m, -24);
+        if (e == 31) return m ? NAN : sgn * INFINITY;
+        return sgn * std::ldexp((double)(m | 1024), e - 25);
+    }
+    default: {
+        uint32_t u = (uint32_t)((const uint16_t*)b)[off] << 16;
+        float f;
+        std::memcpy(&f, &u, 4);
+        return f;
+    }
+    }
+}
+
+
+// ---------------------------------------------------------------------------
+// Adjoint (input and tap gradients of a ROUND_ONCE pass chain)
+// ---------------------------------------------------------------------------
+
+struct AdjPlan {
+    Acc acc;
+    int R;
+    int64_t total;
+    std::vector<CPass> fwd;        // forward passes (zero taps skipped)
+    std::vector<CPass> all;        // every tap, original order (tap gradients)
+    int nF = 0, nB = 0;
+    unsigned nblocks = 0;
+    int maxk = 0;
+    size_t elem_bytes = 0;
+};
+
+static bool float_dtype(int dt) { return dt == NDLGPU_F32 || dt == NDLGPU_F64 || dt == NDLGPU_F16 || dt == NDLGPU_BF16; }
+
+static ndlgpu_status adjoint_prepare(const ndlgpu_view* g, const ndlgpu_view* x, const ndlgpu_view* gx, int npass,
+                                     const ndlgpu_axis_kernel* passes, int border, bool want_taps, int tdt,
+                                     AdjPlan* ap)
+{
+    ndlgpu_status st;
+    if ((st = check_view(g, "grad_out", true)) != NDLGPU_OK) return st;
+    if (x && (st = check_view(x, "src", true)) != NDLGPU_OK) return st;
+    if (gx && (st = check_view(gx, "grad_src", true)) != NDLGPU_OK) return st;
+    if (want_taps && !x) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "tap gradients need the forward input (src)");
+    if (want_taps && tdt != NDLGPU_F32 && tdt != NDLGPU_F64)
+        return fail(NDLGPU_ERR_UNSUPPORTED_DTYPE, "grad_taps must be F32 or F64");
+    if (!float_dtype(g->dtype) || (x && !float_dtype(x->dtype)) || (gx && !float_dtype(gx->dtype)))
+        return fail(NDLGPU_ERR_UNSUPPORTED_DTYPE, "the adjoint takes floating-point images");
+    if (border < NDLGPU_CLAMP || border > NDLGPU_REFLECT) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "unknown border mode");
+    if (x && (st = check_pair(x, g)) != NDLGPU_OK) return st;
+    if (gx && (st = check_pair(g, gx)) != NDLGPU_OK) return st;
+    if (gx && x) {
+        intptr_t a0, a1, b0, b1;
+        view_bytes(x, &a0, &a1);
+        view_bytes(gx, &b0, &b1);
+        if (view_count(x) > 0 && a0 < b1 && b0 < a1) return fail(NDLGPU_ERR_ALIASING, "src and grad_src overlap");
+    }
+    std::vector<LPass> lp;
+    if ((st = lpasses_from(npass, passes, &lp)) != NDLGPU_OK) return st;
+    ap->R = g->rank;
+    ap->total = view_count(g);
+    bool f64 = g->dtype == NDLGPU_F64 || (x && x->dtype == NDLGPU_F64) || (gx && gx->dtype == NDLGPU_F64);
+    ap->acc = f64 ? Acc::F64 : Acc::F32;
+    for (const LPass& p : lp) {
+        if (p.axis < 0 || p.axis >= ap->R) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "pass axis out of range");
+        CPass f, a;
+        f.axis = a.axis = p.axis;
+        for (int k = 0; k < (int)p.taps.size(); k++) {
+            const int o = k - p.center;
+            if (border != NDLGPU_CLAMP && ap->total > 0 && (o > g->extent[p.axis] || o < -g->extent[p.axis]))
+                return fail(NDLGPU_ERR_RADIUS_EXCEEDS_EXTENT, "tap offset exceeds the extent (Wrap/Reflect map one period only)");
+            a.off.push_back(o);
+            a.w.push_back(p.taps[k]);
+            if (p.taps[k] != 0.0) {
+                f.off.push_back(o);
+                f.w.push_back(p.taps[k]);
+            }
+        }
+        ap->maxk = std::max(ap->maxk, (int)a.off.size());
+        ap->fwd.push_back(f);
+        ap->all.push_back(a);
+    }
+    if (ap->total >= (int64_t(1) << 31))
+        return fail(NDLGPU_ERR_INDEX_OVERFLOW, "the adjoint supports images of fewer than 2^31 elements");
+    const int n = (int)lp.size();
+    ap->nF = want_taps ? n - 1 : 0;
+    ap->nB = (n > 1) ? std::min(2, n - 1) : 0;
+    ap->elem_bytes = align_up((size_t)ap->total * dtype_size(acc_dtype(ap->acc)));
+    ap->nblocks = want_taps && ap->total > 0 ? tap_grad_blocks((uint32_t)ap->total) : 0;
+    return NDLGPU_OK;
+}
+
+static size_t adjoint_workspace(const AdjPlan& ap)
+{
+    if (ap.total == 0) return 0;
+    return (size_t)(ap.nF + ap.nB) * ap.elem_bytes + align_up((size_t)ap.nblocks * ap.maxk * sizeof(double));
+}
+
+static ndlgpu_status adjoint_execute(const ndlgpu_view* g, const ndlgpu_view* x, const ndlgpu_view* gx,
+                                     int border, void* grad_taps, int tdt, const AdjPlan& ap, void* ws,
+                                     size_t ws_bytes, cudaStream_t s)
+{
+    if (ap.total == 0) return NDLGPU_OK;
+    Scratch sc;
+    ndlgpu_status st = get_scratch(adjoint_workspace(ap), ws, ws_bytes, s, &sc);
+    if (st != NDLGPU_OK) return st;
+    const int n = (int)ap.fwd.size();
+    const int adt = acc_dtype(ap.acc);
+    Canon geo;   // logical axis order, no flips: the general kernels take any strides
+    geo.total = ap.total;
+    for (int i = 0; i < ap.R; i++) geo.ax.push_back(CAxis{g->extent[i], 0, 0, i});
+    std::vector<int64_t> cst = contiguous_strides(geo);
+    auto strides_of = [&](const ndlgpu_view* v) {
+        std::vector<int64_t> r(ap.R);
+        for (int i = 0; i < ap.R; i++) r[i] = v->stride[i];
+        return r;
+    };
+    char* base = (char*)sc.base;
+    std::vector<char*> F(ap.nF), B(ap.nB);
+    for (int i = 0; i < ap.nF; i++) F[i] = base + (size_t)i * ap.elem_bytes;
+    for (int i = 0; i < ap.nB; i++) B[i] = base + (size_t)(ap.nF + i) * ap.elem_bytes;
+    double* partial = (double*)(base + (size_t)(ap.nF + ap.nB) * ap.elem_bytes);
+    const std::vector<int32_t> none;
+
+    // forward intermediates (inputs of passes 1..n-1)
+    std::vector<const char*> in_ptr(n, nullptr);
+    std::vector<int> in_dt(n, adt);
+    std::vector<std::vector<int64_t>> in_st(n, cst);
+    if (grad_taps) {
+        in_ptr[0] = (const char*)x->data;
+        in_dt[0] = x->dtype;
+        in_st[0] = strides_of(x);
+        for (int p = 0; p + 1 < n; p++) {
+            st = run_generic_pass(ap.acc, geo, ap.fwd[p], in_ptr[p], in_dt[p], in_st[p], F[p], adt, cst, border,
+                                  STORE_CAST, 0, none, s);
+            if (st != NDLGPU_OK) return st;
+            in_ptr[p + 1] = F[p];
+        }
+    }
+    // backward sweep
+    const char* gcur = (const char*)g->data;
+    int gdt = g->dtype;
+    std::vector<int64_t> gst = strides_of(g);
+    size_t tap_off = 0;
+    std::vector<size_t> tap_base(n, 0);
+    for (int p = 0; p < n; p++) { tap_base[p] = tap_off; tap_off += ap.all[p].off.size(); }
+    const int tes = (tdt == NDLGPU_F64) ? 8 : 4;
+    for (int p = n - 1; p >= 0; p--) {
+        if (grad_taps) {
+            TapGradParams tp;
+            std::memset(&tp, 0, sizeof(tp));
+            tp.g = gcur;
+            tp.x = in_ptr[p];
+            tp.partial = partial;
+            tp.g_dtype = gdt;
+            tp.x_dtype = in_dt[p];
+            tp.rank = ap.R;
+            tp.axis = ap.all[p].axis;
+            tp.ntap = (int)ap.all[p].off.size();
+            tp.border = border;
+            tp.total = (uint32_t)ap.total;
+            for (int i = 0; i < ap.R; i++) {
+                tp.n[i] = g->extent[i];
+                tp.gs[i] = gst[i];
+                tp.xs[i] = in_st[p][i];
+                tp.div[i].init((uint32_t)g->extent[i]);
+            }
+            for (int t = 0; t < tp.ntap; t++) tp.off[t] = ap.all[p].off[t];
+            cudaError_t e = launch_tap_grad(ap.acc, tp, ap.nblocks, (char*)grad_taps + tap_base[p] * tes, tdt, s);
+            if (e != cudaSuccess) return cuda_fail(e, "tap gradient");
+        }
+        char* gnext;
+        int ndt;
+        std::vector<int64_t> nst;
+        if (p > 0) {
+            gnext = B[p % 2];
+            ndt = adt;
+            nst = cst;
+        } else if (gx) {
+            gnext = (char*)gx->data;
+            ndt = gx->dtype;
+            nst = strides_of(gx);
+        } else {
+            break;
+        }
+        st = run_generic_pass(ap.acc, geo, ap.fwd[p], gcur, gdt, gst, gnext, ndt, nst, border, STORE_CAST, 0, none, s,
+                              true);
+        if (st != NDLGPU_OK) return st;
+        gcur = gnext;
+        gdt = ndt;
+        gst = nst;
+    }
+    return NDLGPU_OK;
+}
+
+}  // namespace ndlgpu
+
+using namespace ndlgpu;
+
+extern "C" {
+
+const char* ndlgpu_version(void) { return "ndlgpu 0.1.0 (sm_100a)"; }
+
+const char* ndlgpu_status_string(ndlgpu_status s)
+{
+    switch (s) {
+    case NDLGPU_OK: return "ok";
+    case NDLGPU_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case NDLGPU_ERR_UNSUPPORTED_DTYPE: return "unsupported dtype";
+    case NDLGPU_ERR_EXTENT_MISMATCH: return "extent mismatch";
+    case NDLGPU_ERR_RADIUS_EXCEEDS_EXTENT: return "kernel radius exceeds extent";
+    case NDLGPU_ERR_ALIASING: return "src and dst overlap";
+    case NDLGPU_ERR_INDEX_OVERFLOW: return "index overflow";
+    case NDLGPU_ERR_BAD_SIGMA: return "bad sigma";
+    case NDLGPU_ERR_WORKSPACE: return "workspace too small";
+    case NDLGPU_ERR_CUDA: return "CUDA error";
+    case NDLGPU_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case NDLGPU_ERR_TOO_MANY_TAPS: return "too many taps";
+    case NDLGPU_ERR_DEVICE_CHECK: return "device guard fired";
+    }
+    return "unknown status";
+}
+
+const char* ndlgpu_last_error(void) { return t_last_error.c_str(); }
+
+ndlgpu_status ndlgpu_convolve_axes_workspace_size(const ndlgpu_view* src, const ndlgpu_view* dst, int npass,
+                                                  const ndlgpu_axis_kernel* passes, int border, int compose,
+                                                  int precision, size_t* bytes)
+{
+    t_last_error.clear();
+    if (!bytes) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "bytes is NULL");
+    *bytes = 0;
+    std::vector<LPass> lp;
+    ndlgpu_status st = lpasses_from(npass, passes, &lp);
+    if (st != NDLGPU_OK) return st;
+    Canon c;
+    Plan pl;
+    st = prepare(src, dst, lp, border, compose, precision, &c, &pl);
+    if (st != NDLGPU_OK || c.total == 0) return st;
+    *bytes = plan_workspace(c, pl);
+    return NDLGPU_OK;
+}
+
+ndlgpu_status ndlgpu_convolve_axes(const ndlgpu_view* src, const ndlgpu_view* dst, int npass,
+                                   const ndlgpu_axis_kernel* passes, int border, int compose, int precision,
+                                   void* workspace, size_t workspace_bytes, void* stream)
+{
+    t_last_error.clear();
+    std::vector<LPass> lp;
+    ndlgpu_status st = lpasses_from(npass, passes, &lp);
+    if (st != NDLGPU_OK) return st;
+    Canon c;
+    Plan pl;
+    st = prepare(src, dst, lp, border, compose, precision, &c, &pl);
+    if (st != NDLGPU_OK || c.total == 0) return st;
+    return execute(c, pl, compose, border, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+ndlgpu_status ndlgpu_gaussian_blur_workspace_size(const ndlgpu_view* src, const ndlgpu_view* dst, double sigma,
+                                                  int border, size_t* bytes)
+{
+    t_last_error.clear();
+    if (!bytes) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "bytes is NULL");
+    *bytes = 0;
+    std::vector<LPass> lp;
+    ndlgpu_status st = gaussian_passes(src, &sigma, false, &lp);
+    if (st != NDLGPU_OK) return st;
+    Canon c;
+    Plan pl;
+    st = prepare(src, dst, lp, border, NDLGPU_ROUND_ONCE, NDLGPU_PREC_AUTO, &c, &pl);
+    if (st != NDLGPU_OK || c.total == 0) return st;
+    *bytes = plan_workspace(c, pl);
+    return NDLGPU_OK;
+}
+
+ndlgpu_status ndlgpu_gaussian_blur(const ndlgpu_view* src, const ndlgpu_view* dst, double sigma, int border,
+                                   void* workspace, size_t workspace_bytes, void* stream)
+{
+    t_last_error.clear();
+    std::vector<LPass> lp;
+    ndlgpu_status st = gaussian_passes(src, &sigma, false, &lp);
+    if (st != NDLGPU_OK) return st;
+    Canon c;
+    Plan pl;
+    st = prepare(src, dst, lp, border, NDLGPU_ROUND_ONCE, NDLGPU_PREC_AUTO, &c, &pl);
+    if (st != NDLGPU_OK || c.total == 0) return st;
+    return execute(c, pl, NDLGPU_ROUND_ONCE, border, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+ndlgpu_status ndlgpu_gaussian_blur_axes(const ndlgpu_view* src, const ndlgpu_view* dst, const double* sigma_per_axis,
+                                        int border, void* workspace, size_t workspace_bytes, void* stream)
+{
+    t_last_error.clear();
+    if (!sigma_per_axis) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "sigma_per_axis is NULL");
+    std::vector<LPass> lp;
+    ndlgpu_status st = gaussian_passes(src, sigma_per_axis, true, &lp);
+    if (st != NDLGPU_OK) return st;
+    Canon c;
+    Plan pl;
+    st = prepare(src, dst, lp, border, NDLGPU_ROUND_ONCE, NDLGPU_PREC_AUTO, &c, &pl);
+    if (st != NDLGPU_OK || c.total == 0) return st;
+    return execute(c, pl, NDLGPU_ROUND_ONCE, border, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+ndlgpu_status ndlgpu_convolve_ex(const ndlgpu_view* src, const ndlgpu_view* dst, const ndlgpu_view* kernel,
+                                 int border, int precision, void* stream)
+{
+    t_last_error.clear();
+    ndlgpu_status st;
+    if ((st = check_view(src, "src", true)) != NDLGPU_OK) return st;
+    if ((st = check_view(dst, "dst", true)) != NDLGPU_OK) return st;
+    if ((st = check_view(kernel, "kernel", false)) != NDLGPU_OK) return st;
+    if ((st = check_pair(src, dst)) != NDLGPU_OK) return st;
+    if (kernel->rank != src->rank) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "kernel rank must equal image rank");
+    if (border < NDLGPU_CLAMP || border > NDLGPU_REFLECT) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "unknown border mode");
+    if (precision < NDLGPU_PREC_AUTO || precision > NDLGPU_PREC_EXACT)
+        return fail(NDLGPU_ERR_INVALID_ARGUMENT, "unknown precision");
+    const int R = src->rank;
+    int64_t kn = view_count(kernel);
+    if (kn == 0) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "kernel is empty");
+    if (!kernel->data) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "kernel data is NULL");
+    int wide = -1, nwide = 0;
+    for (int i = 0; i < R; i++)
+        if (kernel->extent[i] > 1) { wide = i; nwide++; }
+    if (nwide <= 1) {
+        // a {1,..,K,..,1} kernel: one separable pass (convolution.h:132-139)
+        const int axis = wide < 0 ? 0 : wide;
+        LPass lp;
+        lp.axis = axis;
+        lp.center = (int)(kernel->extent[axis] / 2);   // image/detail.h:161
+        if (kernel->extent[axis] > kMaxTaps) return fail(NDLGPU_ERR_TOO_MANY_TAPS, "kernel has more than 255 taps");
+        for (int64_t k = 0; k < kernel->extent[axis]; k++) lp.taps.push_back(host_value(kernel, k * kernel->stride[axis]));
+        Canon c;
+        Plan pl;
+        st = prepare(src, dst, {lp}, border, NDLGPU_CAST_EACH, precision, &c, &pl);
+        if (st != NDLGPU_OK || c.total == 0) return st;
+        return execute(c, pl, NDLGPU_CAST_EACH, border, nullptr, 0, (cudaStream_t)stream);
+    }
+    // general N-D kernel: nonzero taps in coordinates() order (axis 0 fastest,
+    // image/detail.h:127-143, :164-174), centre K/2 per axis
+    if (view_count(src) == 0) return NDLGPU_OK;
+    std::vector<int32_t> off;
+    std::vector<double> w;
+    std::vector<int64_t> kc(R, 0);
+    for (int64_t t = 0; t < kn; t++) {
+        int64_t ko = 0;
+        for (int i = 0; i < R; i++) ko += kc[i] * kernel->stride[i];
+        const double v = host_value(kernel, ko);
+        if (v != 0.0) {
+            for (int i = 0; i < R; i++) {
+                const int64_t o = kc[i] - kernel->extent[i] / 2;
+                if (border != NDLGPU_CLAMP && (o > src->extent[i] || o < -src->extent[i]))
+                    return fail(NDLGPU_ERR_RADIUS_EXCEEDS_EXTENT, "kernel radius exceeds the image extent (Wrap/Reflect)");
+                off.push_back((int32_t)o);
+            }
+            w.push_back(v);
+        }
+        for (int i = 0; i < R; i++) {
+            if (++kc[i] < kernel->extent[i]) break;
+            kc[i] = 0;
+        }
+    }
+    if ((int64_t)w.size() > NDLGPU_MAX_ND_TAPS) return fail(NDLGPU_ERR_TOO_MANY_TAPS, "more than 4096 nonzero kernel taps");
+    if (view_count(src) >= (int64_t(1) << 31))
+        return fail(NDLGPU_ERR_INDEX_OVERFLOW, "N-D kernels support images of fewer than 2^31 elements");
+    Acc acc = Acc::F64;
+    if (precision == NDLGPU_PREC_FP32) acc = Acc::F32;
+    else if (precision == NDLGPU_PREC_AUTO && !dtype_integral(dst->dtype) && dst->dtype != NDLGPU_F64 &&
+             src->dtype != NDLGPU_F64)
+        acc = Acc::F32;
+    GenericNdParams p;
+    std::memset(&p, 0, sizeof(p));
+    p.src = (const char*)src->data;
+    p.dst = (char*)dst->data;
+    p.src_dtype = src->dtype;
+    p.dst_dtype = dst->dtype;
+    p.rank = R;
+    p.ntap = (int)w.size();
+    p.border = border;
+    p.store_mode = STORE_CAST;
+    p.total = (uint32_t)view_count(src);
+    for (int i = 0; i < R; i++) {
+        p.n[i] = src->extent[i];
+        p.ss[i] = src->stride[i];
+        p.ds[i] = dst->stride[i];
+        p.div[i].init((uint32_t)src->extent[i]);
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    if (w.empty()) {
+        // every tap is zero: convolve() writes DstT(0) everywhere
+        w.push_back(0.0);
+        for (int i = 0; i < R; i++) off.push_back(0);
+        p.ntap = 0;
+    }
+    const size_t ob = align_up(off.size() * sizeof(int32_t));
+    Scratch sc;
+    st = get_scratch(ob + w.size() * sizeof(double), nullptr, 0, s, &sc);
+    if (st != NDLGPU_OK) return st;
+    cudaError_t e = cudaMemcpyAsync(sc.base, off.data(), off.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync((char*)sc.base + ob, w.data(), w.size() * sizeof(double), cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return cuda_fail(e, "tap upload");
+    p.tap_off = (const int32_t*)sc.base;
+    p.tap_w = (const double*)((char*)sc.base + ob);
+    e = launch_generic_nd(acc, p, s);
+    if (e != cudaSuccess) return cuda_fail(e, "N-D kernel");
+    // the pageable-memory copies above completed staging before returning;
+    // the scratch is released stream-ordered after the kernel
+    return NDLGPU_OK;
+}
+
+ndlgpu_status ndlgpu_convolve(const ndlgpu_view* src, const ndlgpu_view* dst, const ndlgpu_view* kernel, int border,
+                              void* stream)
+{
+    return ndlgpu_convolve_ex(src, dst, kernel, border, NDLGPU_PREC_AUTO, stream);
+}
+
+ndlgpu_status ndlgpu_convolve_axes_adjoint_workspace_size(const ndlgpu_view* grad_out, const ndlgpu_view* src,
+                                                          const ndlgpu_view* grad_src, int npass,
+                                                          const ndlgpu_axis_kernel* passes, int border,
+                                                          int grad_taps_dtype, size_t* bytes)
+{
+    t_last_error.clear();
+    if (!bytes) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "bytes is NULL");
+    *bytes = 0;
+    AdjPlan ap;
+    ndlgpu_status st = adjoint_prepare(grad_out, src, grad_src, npass, passes, border, src != nullptr,
+                                       grad_taps_dtype, &ap);
+    if (st != NDLGPU_OK) return st;
+    *bytes = adjoint_workspace(ap);
+    return NDLGPU_OK;
+}
+
+ndlgpu_status ndlgpu_convolve_axes_adjoint(const ndlgpu_view* grad_out, const ndlgpu_view* src,
+                                           const ndlgpu_view* grad_src, int npass, const ndlgpu_axis_kernel* passes,
+                                           int border, void* grad_taps, int grad_taps_dtype, void* workspace,
+                                           size_t workspace_bytes, void* stream)
+{
+    t_last_error.clear();
+    if (!grad_src && !grad_taps) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "nothing to compute: grad_src and grad_taps are NULL");
+    AdjPlan ap;
+    ndlgpu_status st = adjoint_prepare(grad_out, src, grad_src, npass, passes, border, grad_taps != nullptr,
+                                       grad_taps_dtype, &ap);
+    if (st != NDLGPU_OK) return st;
+    return adjoint_execute(grad_out, src, grad_src, border, grad_taps, grad_taps_dtype, ap, workspace,
+                           workspace_bytes, (cudaStream_t)stream);
+}
+
+ndlgpu_status ndlgpu_device_status(void* stream, int32_t* code)
+{
+    t_last_error.clear();
+    if (!code) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "code is NULL");
+    cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
+    e = read_device_status((cudaStream_t)stream, code);
+    if (e != cudaSuccess) return cuda_fail(e, "guard read");
+    return NDLGPU_OK;
+}
+
+}  // extern "C"

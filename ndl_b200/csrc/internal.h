@@ -1,0 +1,181 @@
+// internal.h -- types shared by the host planner (host.cpp) and the kernel
+// launchers (*.cu).  Not part of the public ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/ndlgpu.h"
+
+namespace ndlgpu {
+
+constexpr int kMaxRank = NDLGPU_MAX_RANK;
+constexpr int kMaxTaps = NDLGPU_MAX_TAPS;
+
+// How a pass accumulates.
+//   F32: FP32 fused multiply-add (float storage types).
+//   F64: the reference's exact sequence, total = total + x*w with the
+//        product and the sum each rounded (convolution.h:66-68).
+//   I32: integer numerators of dyadic taps (w = m / 2^shift); exact.
+enum class Acc : int { F32 = 0, F64 = 1, I32 = 2 };
+
+// How an accumulator becomes DstT.
+//   CAST : static_cast<DstT> -- truncation toward zero for integral DstT
+//          (convolution.h:69); round-to-nearest for float DstT.
+//   ROUND: std::round (half away from zero) first for integral DstT
+//          (convolution.h:184).
+//   RAW  : the accumulator itself, into a scratch buffer of the Acc type.
+enum StoreMode : int { STORE_CAST = 0, STORE_ROUND = 1, STORE_RAW = 2 };
+
+inline bool dtype_valid(int dt) { return dt >= NDLGPU_U8 && dt <= NDLGPU_BF16; }
+inline bool dtype_integral(int dt) { return dt >= NDLGPU_U8 && dt <= NDLGPU_U64; }
+inline int dtype_size(int dt)
+{
+    switch (dt) {
+    case NDLGPU_U8: case NDLGPU_I8: return 1;
+    case NDLGPU_U16: case NDLGPU_I16: case NDLGPU_F16: case NDLGPU_BF16: return 2;
+    case NDLGPU_I32: case NDLGPU_U32: case NDLGPU_F32: return 4;
+    default: return 8;
+    }
+}
+inline int acc_dtype(Acc a)
+{
+    return a == Acc::F32 ? NDLGPU_F32 : (a == Acc::F64 ? NDLGPU_F64 : NDLGPU_I32);
+}
+
+// Unsigned 32-bit division by an invariant divisor with a multiply-high
+// (Granlund & Montgomery, "Division by Invariant Integers using
+// Multiplication", PLDI 1994, sec. 4): q = (mulhi(m, n) + n) >> l, evaluated
+// without overflow as (t + ((n - t) >> 1)) >> (l - 1).
+struct FastDiv {
+    uint32_t d;
+    uint32_t m;
+    uint32_t l;
+    void init(uint32_t div)
+    {
+        d = div;
+        l = 0;
+        while (l < 32 && (uint64_t(1) << l) < div) l++;
+        m = (l == 0) ? 0u : uint32_t(((uint64_t(1) << 32) * ((uint64_t(1) << l) - div)) / div + 1);
+    }
+#ifdef __CUDACC__
+    __device__ __forceinline__ uint32_t div(uint32_t n) const
+    {
+        if (l == 0) return n;
+        uint32_t t = __umulhi(m, n);
+        return (t + ((n - t) >> 1)) >> (l - 1);
+    }
+#endif
+    uint32_t div_host(uint32_t n) const
+    {
+        if (l == 0) return n;
+        uint32_t t = uint32_t((uint64_t(m) * n) >> 32);
+        return (t + ((n - t) >> 1)) >> (l - 1);
+    }
+};
+
+// One 1-D pass of the general kernel over a canonical geometry.
+struct GenericPassParams {
+    const char* src;
+    char* dst;
+    int src_dtype;
+    int dst_dtype;
+    int rank;
+    int axis;
+    int ntap;
+    int border;
+    int store_mode;
+    int shift;            // Acc::I32: result = acc / 2^shift
+    uint32_t total;       // outputs in this launch (< 2^32)
+    int64_t n[kMaxRank];
+    int64_t ss[kMaxRank]; // source strides (elements)
+    int64_t ds[kMaxRank]; // destination strides (elements)
+    FastDiv div[kMaxRank];
+    int off[kMaxTaps];    // tap offsets, in summation order
+    double wd[kMaxTaps];
+    float wf[kMaxTaps];
+    int32_t wi[kMaxTaps];
+};
+
+// The general N-D kernel (non-separable convolve()): taps live in device
+// memory as ntap records of rank int32 offsets plus a double weight.
+struct GenericNdParams {
+    const char* src;
+    char* dst;
+    const int32_t* tap_off;  // ntap * rank
+    const double* tap_w;     // ntap
+    int src_dtype;
+    int dst_dtype;
+    int rank;
+    int ntap;
+    int border;
+    int store_mode;
+    uint32_t total;
+    int64_t n[kMaxRank];
+    int64_t ss[kMaxRank];
+    int64_t ds[kMaxRank];
+    FastDiv div[kMaxRank];
+};
+
+cudaError_t launch_generic_pass(Acc acc, const GenericPassParams& p, cudaStream_t s);
+// Transposed pass: p.src = gradient at the pass output, p.dst = input gradient.
+cudaError_t launch_pass_adjoint(Acc acc, const GenericPassParams& p, cudaStream_t s);
+
+// Tap gradients of one pass: dw[t] = sum_i g[i] * x[map(i + off[t])].
+struct TapGradParams {
+    const char* g;
+    const char* x;
+    double* partial;      // [nblocks][ntap]
+    int g_dtype;
+    int x_dtype;
+    int rank;
+    int axis;
+    int ntap;
+    int border;
+    uint32_t total;
+    int64_t n[kMaxRank];
+    int64_t gs[kMaxRank];
+    int64_t xs[kMaxRank];
+    FastDiv div[kMaxRank];
+    int off[kMaxTaps];
+};
+unsigned tap_grad_blocks(uint32_t total);
+cudaError_t launch_tap_grad(Acc acc, const TapGradParams& p, unsigned nblocks, void* out, int out_dtype,
+                            cudaStream_t s);
+cudaError_t launch_generic_nd(Acc acc, const GenericNdParams& p, cudaStream_t s);
+
+// ---------------------------------------------------------------------------
+// Fused separable forward (up to three pass axes, one HBM read + one write).
+// Axis roles: X = canonical axis 0 (smallest source stride), Y and Z = the
+// other pass axes (or extent-1 placeholders), batch = everything else.
+struct FusedParams {
+    const char* src;
+    char* dst;
+    int src_dtype;
+    int dst_dtype;
+    int border;
+    int store_mode;
+    int nx, ny, nz;
+    int64_t sx, sy, sz;   // source strides (sx == 1 on the vector path)
+    int64_t dx, dy, dz;   // destination strides
+    int nbatch;           // product of batch extents (batch axes merged)
+    int64_t sb, db;       // batch strides (merged batch must be affine)
+    int kx, ky, kz;       // taps per axis (1 = no pass)
+    int cx, cy, cz;       // centre = -(offset of tap 0)
+    int shift;            // Acc::I32 total shift
+    int zchunk;           // output planes per CTA along Z
+    float wxf[64], wyf[64], wzf[64];
+    int32_t wxi[64], wyi[64], wzi[64];
+};
+
+// Returns cudaErrorNotSupported when no compiled variant matches.
+cudaError_t launch_fused(Acc acc, const FusedParams& p, cudaStream_t s);
+bool fused_supported(Acc acc, int src_dtype, int dst_dtype, int kx, int ky, int kz);
+
+// Device guard word.
+cudaError_t read_device_status(cudaStream_t s, int32_t* code);
+
+}  // namespace ndlgpu

@@ -1,0 +1,357 @@
+"""numpy front end of the oracle (TEST INFRASTRUCTURE ONLY).
+
+Two checkers live behind this module:
+
+* the plain-C FP64 restatement in ``ndl_oracle.c`` (always available), and
+* the UNMODIFIED reference compiled by ``build_oracle.py`` into
+  ``_ref/libndlref.so`` (available where it was built; ``have_reference()``).
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline legs use
+this module.  The product library never imports it.
+
+Array convention: a numpy array of shape ``(n_{D-1}, ..., n_1, n_0)`` is the
+ndl image of extent ``{n_0, n_1, ..., n_{D-1}}`` -- ndl axis 0 is numpy's last
+axis (ndl's default layout has axis 0 fastest, image/core.h:858-864).  Any
+numpy view (transposed, reversed, strided) is a valid ndl view of the same
+logical content.
+
+bfloat16 has no numpy dtype; such data is carried as ``np.uint16`` bit
+patterns together with an explicit ``dtype_code`` of ``BF16``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+CLAMP, WRAP, REFLECT = 0, 1, 2
+STORE_CAST, STORE_ROUND = 0, 1
+U8, I8, U16, I16, I32, U32, I64, U64, F32, F64, F16, BF16 = range(12)
+
+_NP_CODE = {
+    np.dtype(np.uint8): U8, np.dtype(np.int8): I8, np.dtype(np.uint16): U16,
+    np.dtype(np.int16): I16, np.dtype(np.int32): I32, np.dtype(np.uint32): U32,
+    np.dtype(np.int64): I64, np.dtype(np.uint64): U64, np.dtype(np.float32): F32,
+    np.dtype(np.float64): F64, np.dtype(np.float16): F16,
+}
+_CODE_NP = {v: k for k, v in _NP_CODE.items()}
+_CODE_NP[BF16] = np.dtype(np.uint16)
+
+_lib = None
+_ref = None
+
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_f64p = ctypes.POINTER(ctypes.c_double)
+_i32p = ctypes.POINTER(ctypes.c_int)
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        path = os.path.join(HERE, "libndloracle.so")
+        if not os.path.exists(path):
+            raise RuntimeError("oracle not built: run oracle/build_oracle.py")
+        _lib = ctypes.CDLL(path)
+        for name in ("ora_convolve", "ora_axis_pass", "ora_axis_pass_adjoint", "ora_axis_tap_grad"):
+            getattr(_lib, name).restype = ctypes.c_int
+        _lib.ora_gaussian_weights.restype = ctypes.c_int
+        _lib.ora_gaussian_weights.argtypes = [ctypes.c_double, _f64p]
+        _lib.ora_gaussian_radius.restype = ctypes.c_int
+        _lib.ora_gaussian_radius.argtypes = [ctypes.c_double]
+        _lib.ora_border_map.restype = ctypes.c_int
+        _lib.ora_border_map.argtypes = [ctypes.c_int, ctypes.c_int64, ctypes.c_int64]
+        _lib.ora_cast.restype = ctypes.c_int
+    return _lib
+
+
+def reference_path():
+    return os.path.join(HERE, "_ref", "libndlref.so")
+
+
+def have_reference():
+    return os.path.exists(reference_path())
+
+
+def _load_ref():
+    global _ref
+    if _ref is None:
+        if not have_reference():
+            raise RuntimeError("reference shim not built (oracle/build_oracle.py needs the ndl source tree)")
+        _ref = ctypes.CDLL(reference_path())
+        for name in ("ref_convolve", "ref_gaussian_blur", "ref_compose", "ref_view_probe"):
+            getattr(_ref, name).restype = ctypes.c_int
+    return _ref
+
+
+def dtype_code(a, code=None):
+    if code is not None:
+        return code
+    return _NP_CODE[np.dtype(a.dtype)]
+
+
+def to_f64(a, code=None):
+    """Decode any supported array to float64 (logical content preserved)."""
+    code = dtype_code(a, code)
+    if code == BF16:
+        bits = np.ascontiguousarray(a).astype(np.uint32) << 16
+        return bits.view(np.float32).astype(np.float64)
+    return np.ascontiguousarray(a).astype(np.float64)
+
+
+def _ndl_geom(a):
+    """(extent, stride) in ndl axis order, strides in elements."""
+    item = a.dtype.itemsize
+    ext = list(a.shape[::-1])
+    st = [s // item for s in a.strides[::-1]]
+    return ext, st
+
+
+def _arr64(vals):
+    return (ctypes.c_int64 * len(vals))(*vals)
+
+
+# ----------------------------------------------------------------------------
+# FP64 restatement
+# ----------------------------------------------------------------------------
+
+def border_map(border, M, x):
+    return _load().ora_border_map(border, M, x)
+
+
+def gaussian_radius(sigma):
+    """_kernelSize(sigma), mathHelpers.h:17-18."""
+    return _load().ora_gaussian_radius(float(sigma))
+
+
+def gaussian_weights(sigma):
+    """Normalised taps of processing/convolution.h:116-126."""
+    r = gaussian_radius(sigma)
+    w = np.zeros(2 * r + 1, np.float64)
+    _load().ora_gaussian_weights(float(sigma), w.ctypes.data_as(_f64p))
+    return w
+
+
+def convolve_total(src, kernel, border=CLAMP, code=None):
+    """Double totals of convolve(src, ., kernel, border) (before the DstT
+    cast).  ``kernel`` is a numpy array in the same reversed axis order."""
+    x = to_f64(src, code)
+    k = np.ascontiguousarray(kernel, dtype=np.float64)
+    if k.ndim != x.ndim:
+        raise ValueError("kernel rank must equal image rank")
+    out = np.zeros_like(x)
+    ext, st = _ndl_geom(x)
+    _, ost = _ndl_geom(out)
+    kext = list(k.shape[::-1])
+    rc = _load().ora_convolve(x.ndim, x.ctypes.data_as(_f64p), _arr64(ext), _arr64(st),
+                              out.ctypes.data_as(_f64p), _arr64(ost),
+                              k.ctypes.data_as(_f64p), _arr64(kext), border)
+    if rc != 0:
+        raise RuntimeError("ora_convolve failed")
+    return out
+
+
+def axis_pass_total(x, axis, w, border=CLAMP, center=None):
+    """Double totals of one 1-D pass along ndl axis ``axis`` of a float64
+    array (tap k reads offset k - center; center defaults to K/2)."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    K = len(w)
+    c = K // 2 if center is None else center
+    out = np.zeros_like(x)
+    ext, st = _ndl_geom(x)
+    _, ost = _ndl_geom(out)
+    rc = _load().ora_axis_pass(x.ndim, x.ctypes.data_as(_f64p), _arr64(ext), _arr64(st),
+                               out.ctypes.data_as(_f64p), _arr64(ost),
+                               axis, K, c, w.ctypes.data_as(_f64p), border)
+    if rc != 0:
+        raise RuntimeError("ora_axis_pass failed")
+    return out
+
+
+def axis_pass_adjoint(g, axis, w, border=CLAMP, center=None):
+    g = np.ascontiguousarray(g, dtype=np.float64)
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    K = len(w)
+    c = K // 2 if center is None else center
+    out = np.zeros_like(g)
+    ext, st = _ndl_geom(g)
+    _, ost = _ndl_geom(out)
+    rc = _load().ora_axis_pass_adjoint(g.ndim, g.ctypes.data_as(_f64p), _arr64(ext), _arr64(st),
+                                       out.ctypes.data_as(_f64p), _arr64(ost),
+                                       axis, K, c, w.ctypes.data_as(_f64p), border)
+    if rc != 0:
+        raise RuntimeError("ora_axis_pass_adjoint failed")
+    return out
+
+
+def axis_tap_grad(g, x, axis, K, border=CLAMP, center=None):
+    g = np.ascontiguousarray(g, dtype=np.float64)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    c = K // 2 if center is None else center
+    out = np.zeros(K, np.float64)
+    ext, st = _ndl_geom(g)
+    _, xst = _ndl_geom(x)
+    rc = _load().ora_axis_tap_grad(g.ndim, g.ctypes.data_as(_f64p), _arr64(ext), _arr64(st),
+                                   x.ctypes.data_as(_f64p), _arr64(xst),
+                                   axis, K, c, border, out.ctypes.data_as(_f64p))
+    if rc != 0:
+        raise RuntimeError("ora_axis_tap_grad failed")
+    return out
+
+
+def cast(total, out_code, mode=STORE_CAST):
+    """DstT conversion of double totals: static_cast (convolution.h:69) or
+    std::round-then-cast for integral DstT (convolution.h:184)."""
+    t = np.ascontiguousarray(total, dtype=np.float64)
+    out = np.empty(t.shape, _CODE_NP[out_code])
+    rc = _load().ora_cast(t.ctypes.data_as(_f64p), ctypes.c_int64(t.size), out_code, mode,
+                          out.ctypes.data_as(ctypes.c_void_p))
+    if rc != 0:
+        raise RuntimeError("ora_cast failed")
+    return out
+
+
+def compose(src, passes, border=CLAMP, out_code=F32, mode=STORE_ROUND, code=None):
+    """Oracle of a per-axis separable composition.
+
+    passes: list of (ndl_axis, taps) applied in order.
+    mode STORE_ROUND: gaussian_blur's structure (processing/convolution.h:
+      148-185): double intermediates, one final round (integral) / cast.
+      A single pass is a plain convolve() (truncating cast), as in
+      gaussian_blur's DIM==1 branch (:141-146).
+    mode STORE_CAST: every pass is a full convolve() into DstT (the chain of
+      separate convolve() calls).
+    """
+    x = to_f64(src, code)
+    if len(passes) == 1:
+        ax, w = passes[0]
+        return cast(axis_pass_total(x, ax, w, border), out_code, STORE_CAST)
+    if mode == STORE_CAST:
+        cur = x
+        for ax, w in passes:
+            cur = cast(axis_pass_total(cur, ax, w, border), out_code, STORE_CAST)
+            cur = to_f64(cur, out_code)
+        return cast(cur, out_code, STORE_CAST)
+    cur = x
+    for ax, w in passes:
+        cur = axis_pass_total(cur, ax, w, border)
+    return cast(cur, out_code, STORE_ROUND)
+
+
+def compose_total(src, passes, border=CLAMP, code=None):
+    """Double result of the composition before any final cast."""
+    cur = to_f64(src, code)
+    for ax, w in passes:
+        cur = axis_pass_total(cur, ax, w, border)
+    return cur
+
+
+def gaussian_blur(src, sigma, border=CLAMP, out_code=None, code=None):
+    """gaussian_blur(src, dst, sigma, border), processing/convolution.h:107-186."""
+    w = gaussian_weights(sigma)
+    if out_code is None:
+        out_code = dtype_code(src, code)
+    ndim = np.asarray(src).ndim
+    return compose(src, [(a, w) for a in range(ndim)], border, out_code, STORE_ROUND, code)
+
+
+def compose_adjoint(g, x, passes, border=CLAMP):
+    """FP64 adjoint of the composition Y = P_n(...P_1(X)) for
+    L = sum(g * Y): returns (dL/dX, [dL/dw_p for each pass])."""
+    inputs = [np.ascontiguousarray(x, dtype=np.float64)]
+    for ax, w in passes[:-1]:
+        inputs.append(axis_pass_total(inputs[-1], ax, w, border))
+    gcur = np.ascontiguousarray(g, dtype=np.float64)
+    tap = [None] * len(passes)
+    for p in range(len(passes) - 1, -1, -1):
+        ax, w = passes[p]
+        tap[p] = axis_tap_grad(gcur, inputs[p], ax, len(w), border)
+        gcur = axis_pass_adjoint(gcur, ax, w, border)
+    return gcur, tap
+
+
+# ----------------------------------------------------------------------------
+# The compiled reference (oracle/_ref)
+# ----------------------------------------------------------------------------
+
+def _i32arr(vals):
+    return (ctypes.c_int * len(vals))(*[int(v) for v in vals])
+
+
+def ref_convolve(src, kernel, border=CLAMP, out_dtype=None, out=None):
+    """Runs ndl::convolve() itself.  ``out`` may be a preallocated view."""
+    lib = _load_ref()
+    if out is None:
+        out = np.zeros(src.shape, out_dtype or src.dtype)
+    k = np.ascontiguousarray(kernel, dtype=np.float64)
+    ext, sst = _ndl_geom(src)
+    _, dst = _ndl_geom(out)
+    rc = lib.ref_convolve(src.ndim, dtype_code(src), ctypes.c_void_p(src.ctypes.data), _i32arr(ext), _i32arr(sst),
+                          dtype_code(out), ctypes.c_void_p(out.ctypes.data), _i32arr(dst),
+                          k.ctypes.data_as(_f64p), _i32arr(list(k.shape[::-1])), border)
+    if rc != 0:
+        raise RuntimeError("ref_convolve failed (%d)" % rc)
+    return out
+
+
+def ref_gaussian_blur(src, sigma, border=CLAMP, out_dtype=None, out=None):
+    lib = _load_ref()
+    if out is None:
+        out = np.zeros(src.shape, out_dtype or src.dtype)
+    ext, sst = _ndl_geom(src)
+    _, dst = _ndl_geom(out)
+    rc = lib.ref_gaussian_blur(src.ndim, dtype_code(src), ctypes.c_void_p(src.ctypes.data), _i32arr(ext), _i32arr(sst),
+                               dtype_code(out), ctypes.c_void_p(out.ctypes.data), _i32arr(dst),
+                               ctypes.c_double(sigma), border)
+    if rc != 0:
+        raise RuntimeError("ref_gaussian_blur failed (%d)" % rc)
+    return out
+
+
+def ref_compose(src, passes, border=CLAMP, out_dtype=None, mode=STORE_ROUND, out=None):
+    """Reference convolve() calls composed per axis (ref_shim.cpp:ref_compose);
+    mode STORE_ROUND = gaussian_blur structure, STORE_CAST = convolve chain."""
+    lib = _load_ref()
+    if out is None:
+        out = np.zeros(src.shape, out_dtype or src.dtype)
+    ext, sst = _ndl_geom(src)
+    _, dst = _ndl_geom(out)
+    axes = [int(a) for a, _ in passes]
+    ntaps = [len(w) for _, w in passes]
+    taps = np.concatenate([np.asarray(w, np.float64) for _, w in passes])
+    rc = lib.ref_compose(src.ndim, dtype_code(src), ctypes.c_void_p(src.ctypes.data), _i32arr(ext), _i32arr(sst),
+                         dtype_code(out), ctypes.c_void_p(out.ctypes.data), _i32arr(dst),
+                         len(passes), _i32arr(axes), _i32arr(ntaps), taps.ctypes.data_as(_f64p),
+                         0 if mode == STORE_ROUND else 1, border)
+    if rc != 0:
+        raise RuntimeError("ref_compose failed (%d)" % rc)
+    return out
+
+
+def ref_view_probe(base_extent, ops):
+    """Runs the reference's Image view builders; ops are tuples
+    ('swap', a, b) | ('mirror', a) | ('view', axis, start, end, step).
+    Returns (element offset, extent, stride) in ndl axis order."""
+    lib = _load_ref()
+    enc = []
+    for op in ops:
+        if op[0] == "swap":
+            enc += [1, op[1], op[2]]
+        elif op[0] == "mirror":
+            enc += [2, op[1], 0]
+        elif op[0] == "view":
+            enc += [3, op[1], 0, 4, op[2], op[3], 5, op[4], 0]
+        else:
+            raise ValueError(op)
+    dim = len(base_extent)
+    off = ctypes.c_longlong(0)
+    ext = (ctypes.c_int * dim)()
+    st = (ctypes.c_int * dim)()
+    rc = lib.ref_view_probe(dim, _i32arr(base_extent), _i32arr(enc), len(enc) // 3,
+                            ctypes.byref(off), ext, st)
+    if rc != 0:
+        raise RuntimeError("ref_view_probe failed (%d)" % rc)
+    return off.value, list(ext), list(st)

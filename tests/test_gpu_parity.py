@@ -1,0 +1,368 @@
+"""Parity of the sm_100a kernels (through the C ABI) with the reference.
+
+Checks against (a) golden fixtures the compiled reference produced
+(tests/golden, made by make_golden.py) and (b) the FP64 oracle on seeded
+inputs, over every border mode, element type, view layout and the edge cases
+the reference's tests touch (tiny and ragged extents, extent-1 axes, empty
+images, negative strides).
+
+Tolerances: integral results bit-exact; FP64 and EXACT-precision results
+bit-exact; FP32 results within 1e-6 of the reference relative to the
+magnitude of the stencil sum, |gpu - ref| <= 1e-6 * (|w| * |x|)(i), which is
+the plain 1e-6 relative error wherever data and weights are positive;
+bf16/f16 storage within 4e-3 relative to that same magnitude.
+"""
+import numpy as np
+import pytest
+import torch
+
+import ndl_b200 as n
+from ndl_b200 import BorderMode, Image, abi
+from oracle import oracle as O
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+DEV = "cuda"
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(DEV)
+
+
+def host(t):
+    t = t.detach()
+    if t.dtype == torch.bfloat16:
+        return t.contiguous().view(torch.int16).cpu().numpy().view(np.uint16)
+    return t.cpu().numpy()
+
+
+def magnitude(x, passes, border):
+    """(|w| * |x|): the stencil sum of absolute values, per output."""
+    ax = np.abs(O.to_f64(x))
+    return O.compose_total(ax, [(a, np.abs(np.asarray(w, np.float64))) for a, w in passes], border)
+
+
+def assert_close(got, ref, mag, tol, what=""):
+    got = np.asarray(got, np.float64)
+    ref = np.asarray(ref, np.float64)
+    err = np.abs(got - ref)
+    bound = tol * mag + 1e-30
+    bad = err > bound
+    assert not bad.any(), "%s: %d mismatches, worst err %.3g vs bound %.3g" % (
+        what, bad.sum(), (err / bound).max(), bound.flat[np.argmax(err / bound)])
+
+
+# ---------------------------------------------------------------------------
+# Golden fixtures from the compiled reference
+# ---------------------------------------------------------------------------
+
+@pytest.mark.parametrize("border", [0, 1, 2])
+@pytest.mark.parametrize("sigma", [2.0, 1.3])
+def test_golden_gaussian_f32(border, sigma):
+    d, _ = golden("gauss2d_f32")
+    src = d["src"]
+    s = Image.from_tensor(dev(src))
+    o = Image.empty(s.extent(), torch.float32)
+    n.gaussian_blur(s, o, sigma, border)
+    ref = d["out_b%d_s%s" % (border, str(sigma).replace(".", "p"))]
+    w = O.gaussian_weights(sigma)
+    assert_close(host(o.tensor()), ref, magnitude(src, [(0, w), (1, w)], border), 1e-6, "gaussian f32")
+
+
+@pytest.mark.parametrize("border", [0, 1, 2])
+def test_golden_gaussian_u8_exact(border):
+    # non-dyadic weights: the reference's double sequence, bit-exact
+    d, _ = golden("u8_gauss_s1p5")
+    s = Image.from_tensor(dev(d["src"]))
+    o = Image.empty(s.extent(), torch.uint8)
+    n.gaussian_blur(s, o, 1.5, border)
+    assert (host(o.tensor()) == d["out_b%d" % border]).all()
+
+
+@pytest.mark.parametrize("dst_layout", ["contiguous", "same_view"])
+def test_golden_u8_binomial_view(dst_layout):
+    d, _ = golden("u8_binomial_view")
+    base = dev(d["base"])
+    src = Image.from_tensor(base).swap_axes(0, 2).mirror(1)
+    assert src.stride()[1] < 0
+    w = d["taps"]
+    passes = [(0, w), (1, w), (2, w)]
+    for mode, key in ((abi.ROUND_ONCE, "round_once"), (abi.CAST_EACH, "cast_each")):
+        if dst_layout == "contiguous":
+            dst = Image.empty(src.extent(), torch.uint8)
+        else:
+            dst = Image.from_tensor(torch.zeros_like(base)).swap_axes(0, 2).mirror(1)
+        n.convolve_axes(src, dst, passes, BorderMode.Wrap, compose=mode)
+        assert (host(dst.tensor()) == d[key]).all(), key
+
+
+def test_golden_unit_known_answers():
+    d, _ = golden("unit_known_answers")
+    img = Image.from_tensor(dev(d["img"]))
+    for b in (0, 1, 2):
+        for kk, key in ((np.ones((3, 3), np.int32), "sum3_b%d" % b), (np.ones((5, 5), np.int32), "sum5_b%d" % b)):
+            out = Image.zeros(img.extent(), torch.int32)
+            n.convolve(img, out, kk, b)
+            assert (host(out.tensor()) == d[key]).all(), key
+    i54 = Image.from_tensor(dev(d["img54"]))
+    out = Image.zeros(i54.extent(), torch.int32)
+    n.convolve(i54, out, d["kb"], BorderMode.Wrap)
+    assert (host(out.tensor()) == d["composite_wrap"]).all()
+    assert host(out.tensor()).sum() == d["kb"].sum() * d["img54"].sum()
+    f = Image.from_tensor(dev(d["fimg"]))
+    out = Image.zeros(f.extent(), torch.float64)
+    n.convolve(f, out, d["fk"], BorderMode.Wrap)
+    assert (host(out.tensor()) == d["fft_wrap"]).all()     # FP64: bit-exact
+
+
+def test_golden_one_d():
+    d, _ = golden("one_d")
+    a = Image.from_tensor(dev(d["a"]))
+    out = Image.zeros(a.extent(), torch.float32)
+    n.convolve(a, out, d["box"], BorderMode.Clamp)
+    got = host(out.tensor())
+    # EXPECT_FLOAT_EQ in type_coverage_tests.cpp:148 (4 ulps)
+    assert abs(float(got[1]) - (3.0 + 5.0 + 7.0) / 3.0) <= 4 * np.spacing(np.float32(5.0))
+    assert np.allclose(got, d["out_box"], rtol=1e-6, atol=0)
+    x6 = Image.from_tensor(dev(d["x6"]))
+    o6 = Image.zeros(x6.extent(), torch.uint8)
+    n.gaussian_blur(x6, o6, 2.0, BorderMode.Reflect)      # DIM == 1: truncating convolve()
+    assert (host(o6.tensor()) == d["out_g1"]).all()
+
+
+def test_golden_rand9_reflect_fused():
+    d, _ = golden("f32_rand9_reflect")
+    t = d["taps"]
+    passes = [(0, t[0]), (1, t[1]), (2, t[2])]
+    s = Image.from_tensor(dev(d["src"]))
+    o = Image.empty(s.extent(), torch.float32)
+    n.convolve_axes(s, o, passes, BorderMode.Reflect)
+    assert_close(host(o.tensor()), d["out_f64"], magnitude(d["src"], passes, 2), 1e-6, "rand9")
+    # EXACT precision reproduces the reference's float result bit for bit
+    o2 = Image.empty(s.extent(), torch.float32)
+    n.convolve_axes(s, o2, passes, BorderMode.Reflect, precision=abi.PREC_EXACT)
+    assert (host(o2.tensor()) == d["out"]).all()
+
+
+def test_golden_video4d():
+    d, _ = golden("video4d_f32")
+    s = Image.from_tensor(dev(d["src"]))
+    o = Image.empty(s.extent(), torch.float32)
+    n.gaussian_blur_axes(s, o, [2.5, 2.5, 0.0, 1.5], BorderMode.Reflect)
+    gx, gt = O.gaussian_weights(2.5), O.gaussian_weights(1.5)
+    mag = magnitude(d["src"], [(0, gx), (1, gx), (3, gt)], 2)
+    assert_close(host(o.tensor()), d["out_f64"], mag, 1e-6, "video f32")
+    for tdt, tol in ((torch.bfloat16, 4e-3), (torch.float16, 4e-3)):
+        sb = Image.from_tensor(dev(d["src"]).to(tdt))
+        ob = Image.empty(s.extent(), tdt)
+        n.gaussian_blur_axes(sb, ob, [2.5, 2.5, 0.0, 1.5], BorderMode.Reflect)
+        xin = host(sb.tensor())
+        code = O.BF16 if tdt == torch.bfloat16 else O.F16
+        ref = O.compose_total(O.to_f64(xin, code), [(0, gx), (1, gx), (3, gt)], 2)
+        got = O.to_f64(host(ob.tensor()), code)
+        assert_close(got, ref, mag, tol, str(tdt))
+
+
+def test_golden_u8_trunc_axis():
+    d, _ = golden("u8_trunc_axis")
+    s = Image.from_tensor(dev(d["src"]))
+    for ax in range(3):
+        kshape = [1, 1, 1]
+        kshape[2 - ax] = 5
+        o = Image.zeros(s.extent(), torch.uint8)
+        n.convolve(s, o, d["taps"].reshape(kshape), BorderMode.Reflect)
+        assert (host(o.tensor()) == d["ax%d" % ax]).all(), ax
+
+
+# ---------------------------------------------------------------------------
+# Seeded cases against the FP64 oracle
+# ---------------------------------------------------------------------------
+
+def rand_array(rng, shape, dt):
+    if dt in (np.uint8,):
+        return rng.integers(0, 256, shape).astype(dt)
+    if dt in (np.int16,):
+        return rng.integers(-300, 300, shape).astype(dt)
+    if dt in (np.int32,):
+        return rng.integers(-100000, 100000, shape).astype(dt)
+    return rng.standard_normal(shape).astype(dt)
+
+
+SHAPES_3D = [(1, 1, 1), (5, 3, 2), (9, 13, 17), (33, 70, 65), (40, 31, 130), (3, 97, 5)]
+
+
+@pytest.mark.parametrize("shape", SHAPES_3D)
+@pytest.mark.parametrize("border", [0, 1, 2])
+def test_f32_three_axes_vs_oracle(shape, border):
+    rng = np.random.default_rng(hash((shape, border)) % 2**32)
+    x = rand_array(rng, shape, np.float32)
+    passes = []
+    for ax in range(3):
+        K = 2 * min(4, shape[2 - ax]) + 1 if border != 0 else 9
+        w = rng.standard_normal(K)
+        passes.append((ax, w / np.abs(w).sum()))
+    s = Image.from_tensor(dev(x))
+    o = Image.empty(s.extent(), torch.float32)
+    n.convolve_axes(s, o, passes, border)
+    ref = O.compose_total(x, passes, border)
+    assert_close(host(o.tensor()), ref, magnitude(x, passes, border), 1e-6, "f32 3-axis %s" % (shape,))
+    # the EXACT path is the reference's own sequence, bit for bit
+    o2 = Image.empty(s.extent(), torch.float32)
+    n.convolve_axes(s, o2, passes, border, precision=abi.PREC_EXACT)
+    assert (host(o2.tensor()) == O.cast(ref, O.F32)).all()
+
+
+@pytest.mark.parametrize("border", [0, 1, 2])
+@pytest.mark.parametrize("mode", [abi.ROUND_ONCE, abi.CAST_EACH])
+def test_u8_binomial_vs_oracle_ragged(border, mode):
+    rng = np.random.default_rng(border * 7 + mode)
+    for shape in [(3, 5, 7), (17, 64, 33), (70, 9, 129)]:
+        x = rand_array(rng, shape, np.uint8)
+        w = np.array([1, 4, 6, 4, 1]) / 16.0
+        passes = [(0, w), (1, w), (2, w)]
+        s = Image.from_tensor(dev(x))
+        o = Image.empty(s.extent(), torch.uint8)
+        n.convolve_axes(s, o, passes, border, compose=mode)
+        ref = O.compose(x, passes, border, O.U8, O.STORE_ROUND if mode == abi.ROUND_ONCE else O.STORE_CAST)
+        assert (host(o.tensor()) == ref).all(), shape
+
+
+@pytest.mark.parametrize("dt", [np.uint8, np.int16, np.int32, np.float64])
+@pytest.mark.parametrize("border", [0, 1, 2])
+def test_exact_types_gaussian(dt, border):
+    rng = np.random.default_rng(11)
+    x = rand_array(rng, (21, 30), dt)
+    s = Image.from_tensor(dev(x))
+    o = Image.zeros(s.extent(), torch.from_numpy(x).dtype)
+    n.gaussian_blur(s, o, 1.7, border)
+    ref = O.gaussian_blur(x, 1.7, border)
+    assert (host(o.tensor()) == ref).all()
+
+
+@pytest.mark.parametrize("ops", [
+    [("mirror", 0)],
+    [("swap", 0, 1)],
+    [("swap", 0, 2), ("mirror", 1)],
+    [("view", 0, 1, -2, 2)],
+    [("view", 1, 0, -1, -3), ("swap", 1, 2)],
+])
+@pytest.mark.parametrize("dt", [np.float32, np.uint8])
+def test_views_vs_oracle(ops, dt):
+    rng = np.random.default_rng(3)
+    base = rand_array(rng, (12, 23, 40), dt)
+    t = dev(base)
+    src = Image.from_tensor(t)
+    npv = base
+    for op in ops:
+        if op[0] == "swap":
+            src = src.swap_axes(op[1], op[2])
+            a, b = npv.ndim - 1 - op[1], npv.ndim - 1 - op[2]
+            npv = np.swapaxes(npv, a, b)
+        elif op[0] == "mirror":
+            src = src.mirror(op[1])
+            npv = np.flip(npv, npv.ndim - 1 - op[1])
+        else:
+            _, ax, s0, e0, st = op
+            start = [0, 0, 0]
+            end = [-1, -1, -1]
+            step = [1, 1, 1]
+            start[ax], end[ax], step[ax] = s0, e0, st
+            src = src.view(start, end, step)
+            na = npv.ndim - 1 - ax
+            L = npv.shape[na]
+            s1 = s0 % L if s0 < 0 else s0
+            e1 = e0 % L if e0 < 0 else e0
+            sl = [slice(None)] * npv.ndim
+            sl[na] = slice(s1, e1 + 1, st) if st > 0 else slice(e1, s1 - 1 if s1 > 0 else None, st)
+            npv = npv[tuple(sl)]
+    assert list(src.tensor().shape) == list(npv.shape)
+    assert (host(src.tensor()) == npv).all()
+    w = np.array([1, 4, 6, 4, 1]) / 16.0 if dt == np.uint8 else np.array([0.2, -0.1, 0.5, 0.3, 0.1])
+    passes = [(0, w), (1, w), (2, w)]
+    for border in (0, 1, 2):
+        o = Image.empty(src.extent(), torch.from_numpy(base).dtype)
+        n.convolve_axes(src, o, passes, border)
+        if dt == np.uint8:
+            assert (host(o.tensor()) == O.compose(npv, passes, border, O.U8)).all()
+        else:
+            assert_close(host(o.tensor()), O.compose_total(npv, passes, border), magnitude(npv, passes, border),
+                         1e-6, "view")
+
+
+def test_extent_one_axes_and_single_tap():
+    rng = np.random.default_rng(1)
+    x = rand_array(rng, (1, 7, 1), np.float32)
+    s = Image.from_tensor(dev(x))
+    for border in (0, 1, 2):
+        passes = [(0, [0.25, 0.5, 0.25]), (1, [0.3, 0.4, 0.3]), (2, [1.0])]
+        o = Image.empty(s.extent(), torch.float32)
+        n.convolve_axes(s, o, passes, border)
+        ref = O.compose_total(x, passes, border)
+        assert_close(host(o.tensor()), ref, magnitude(x, passes, border), 1e-6, "extent-1")
+
+
+def test_empty_image():
+    s = Image.empty([0, 4], torch.float32)
+    o = Image.empty([0, 4], torch.float32)
+    n.gaussian_blur(s, o, 1.0)
+    torch.cuda.synchronize()
+
+
+def test_nd_kernel_float_and_zero_taps():
+    rng = np.random.default_rng(2)
+    x = rand_array(rng, (19, 26), np.float32)
+    k = rng.standard_normal((3, 5))
+    k[1, 2] = 0.0
+    s = Image.from_tensor(dev(x))
+    for border in (0, 1, 2):
+        o = Image.empty(s.extent(), torch.float32)
+        n.convolve(s, o, k, border)
+        ref = O.convolve_total(x, k, border)
+        mag = O.convolve_total(np.abs(x), np.abs(k), border)
+        assert_close(host(o.tensor()), ref, mag, 1e-6, "nd")
+        o2 = Image.empty(s.extent(), torch.float32)
+        n.convolve(s, o2, k, border, precision=abi.PREC_EXACT)
+        assert (host(o2.tensor()) == O.cast(ref, O.F32)).all()
+
+
+def test_workspace_given_by_caller():
+    rng = np.random.default_rng(4)
+    x = rand_array(rng, (20, 30, 40), np.float64)
+    s = Image.from_tensor(dev(x))
+    o = Image.empty(s.extent(), torch.float64)
+    w = [0.1, 0.2, 0.4, 0.2, 0.1]
+    passes = [(0, w), (1, w), (2, w)]
+    nb = n.convolve_axes_workspace_size(s, o, passes)
+    assert nb >= 2 * x.size * 8
+    ws = torch.empty(nb, dtype=torch.uint8, device=DEV)
+    n.convolve_axes(s, o, passes, workspace=ws)
+    assert (host(o.tensor()) == O.compose_total(x, passes, 0)).all()
+
+
+# ---------------------------------------------------------------------------
+# Adjoint
+# ---------------------------------------------------------------------------
+
+@pytest.mark.parametrize("border", [0, 1, 2])
+@pytest.mark.parametrize("dt", [np.float64, np.float32])
+def test_adjoint_vs_fp64_oracle(border, dt):
+    rng = np.random.default_rng(17 + border)
+    shape = (11, 14, 17)
+    x = rand_array(rng, shape, dt)
+    g = rand_array(rng, shape, dt)
+    passes = []
+    for ax in range(3):
+        w = rng.standard_normal(9 if border == 0 or ax > 0 else 7)
+        passes.append((ax, w / np.abs(w).sum()))
+    gx_ref, taps_ref = O.compose_adjoint(g, x, passes, border)
+    tg = torch.zeros(sum(len(w) for _, w in passes), dtype=torch.float64, device=DEV)
+    gxi = Image.empty(list(shape[::-1]), torch.from_numpy(x).dtype)
+    n.convolve_axes_adjoint(Image.from_tensor(dev(g)), Image.from_tensor(dev(x)), gxi, passes, border, tg)
+    got = host(gxi.tensor()).astype(np.float64)
+    tol = 1e-12 if dt == np.float64 else 2e-6
+    scale = np.abs(gx_ref).max()
+    assert np.abs(got - gx_ref).max() <= tol * scale * 10
+    tref = np.concatenate(taps_ref)
+    tscale = np.abs(tref).max()
+    assert np.abs(host(tg) - tref).max() <= tol * tscale * 100

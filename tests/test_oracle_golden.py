@@ -1,0 +1,185 @@
+"""The oracle pinned to the reference: known answers of the reference's own
+unit tests, golden fixtures made by the compiled reference, and (where it is
+built) the compiled reference itself on seeded cases."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from conftest import golden
+
+
+def _i32(total):
+    return O.cast(total, O.I32)
+
+
+def test_known_answers_4x4():
+    # unitTests/image_convolution_tests.cpp:18-66
+    img = np.arange(1, 17, dtype=np.int32).reshape(4, 4)
+    ident = np.array([[0, 0, 0], [0, 1, 0], [0, 0, 0]], np.int32)
+    assert (_i32(O.convolve_total(img, ident)) == img).all()
+    s3 = np.ones((3, 3), np.int32)
+    out = _i32(O.convolve_total(img, s3, O.CLAMP))
+    assert out[1, 1] == 1 + 2 + 3 + 5 + 6 + 7 + 9 + 10 + 11
+    assert out[0, 0] == 4 * img[0, 0] + 2 * img[0, 1] + 2 * img[1, 0] + img[1, 1]
+    wrap = _i32(O.convolve_total(img, s3, O.WRAP))
+    assert wrap[0, 0] != out[0, 0]
+    s5 = np.ones((5, 5), np.int32)
+    assert _i32(O.convolve_total(img, s5, O.REFLECT))[0, 0] != _i32(O.convolve_total(img, s5, O.CLAMP))[0, 0]
+
+
+def test_known_answers_demo_grid():
+    # demo/convolution/convolution.cpp:200-240: 5x5 grid 1..25, 3x3 ones
+    grid = np.arange(1, 26, dtype=np.int32).reshape(5, 5)
+    s3 = np.ones((3, 3), np.int32)
+    assert _i32(O.convolve_total(grid, s3))[2, 2] == 117
+    assert _i32(O.convolve_total(grid, s3, O.CLAMP))[0, 0] == 27
+    assert _i32(O.convolve_total(grid, s3, O.WRAP))[0, 0] == 99
+    assert _i32(O.convolve_total(grid, s3, O.REFLECT))[0, 0] == 27
+
+
+def test_composite_wrap_sum_identity():
+    # unitTests/composite_tests.cpp:105-133
+    img = np.arange(1, 21, dtype=np.int32).reshape(4, 5)
+    k = np.array([[1, 2, 1], [2, 4, 2], [1, 2, 1]], np.int32)
+    out = _i32(O.convolve_total(img, k, O.WRAP))
+    assert out.sum() == k.sum() * img.sum()
+
+
+def test_fft_correlation_convention():
+    # unitTests/fft_tests.cpp:164-223: circular cross-correlation (unflipped,
+    # centred at K/2) equals convolve(Wrap) to 1e-6
+    W, H = 16, 8
+    img = np.array([((i + 1) * 37) % 251 for i in range(W * H)], np.float64).reshape(H, W)
+    k = np.array([[1, 2, 1], [0, 1, 0], [-1, 0, 2]], np.float64)
+    out = O.convolve_total(img, k, O.WRAP)
+    pad = np.zeros((H, W))
+    for ky in range(3):
+        for kx in range(3):
+            pad[(ky - 1) % H, (kx - 1) % W] = k[ky, kx]
+    corr = np.real(np.fft.ifft2(np.conj(np.fft.fft2(pad)) * np.fft.fft2(img)))
+    assert np.abs(corr - out).max() < 1e-6
+
+
+def test_float_box_1d():
+    # unitTests/type_coverage_tests.cpp:141-149
+    a = np.array([3, 5, 7, 9], np.float32)
+    out = O.cast(O.convolve_total(a, np.full(3, 1.0 / 3.0), O.CLAMP), O.F32)
+    assert out[1] == np.float32((3.0 + 5.0 + 7.0) / 3.0)
+
+
+def test_border_maps():
+    # unitTests/image_core_tests.cpp:456-508 (4-wide)
+    assert O.border_map(O.CLAMP, 4, -2) == 0
+    assert O.border_map(O.WRAP, 4, -2) == 2
+    assert O.border_map(O.REFLECT, 4, -2) == 1
+    assert O.border_map(O.CLAMP, 4, 5) == 3
+    assert O.border_map(O.WRAP, 4, 5) == 1
+    assert O.border_map(O.REFLECT, 4, 5) == 2
+
+
+def test_gaussian_impulse_response():
+    # docs/tutorials/convolution_tutorial.md:138-150: gaussian_blur(impulse,
+    # response, 1.0) of a 1000 impulse, printed to 2 decimals
+    imp = np.zeros((11, 11))
+    imp[5, 5] = 1000.0
+    r = O.gaussian_blur(imp, 1.0)
+    row5 = [0.00, 0.00, 1.77, 21.55, 96.58, 159.24, 96.58, 21.55, 1.77, 0.00, 0.00]
+    row3 = [0.00, 0.00, 0.24, 2.92, 13.07, 21.55, 13.07, 2.92, 0.24, 0.00, 0.00]
+    assert np.allclose(np.round(r[5], 2), row5)
+    assert np.allclose(np.round(r[3], 2), row3)
+    assert O.gaussian_radius(1.0) == 3 and O.gaussian_radius(2.0) == 6 and O.gaussian_radius(6.0) == 18
+
+
+@pytest.mark.parametrize("name", ["gauss2d_f32", "u8_gauss_s1p5"])
+def test_oracle_matches_golden_gaussian(name):
+    d, meta = golden(name)
+    src = d["src"]
+    for key in d.files:
+        if not key.startswith("out_b"):
+            continue
+        b = int(key[5])
+        sig = meta.get("sigma")
+        if sig is None:
+            sig = float(key.split("_s")[1].replace("p", "."))
+        ours = O.gaussian_blur(src, sig, b)
+        assert ours.dtype == d[key].dtype
+        assert (ours == d[key]).all(), key
+
+
+def test_oracle_matches_golden_u8_view():
+    d, meta = golden("u8_binomial_view")
+    view = d["base"].transpose(2, 1, 0)[:, ::-1, :]
+    w = d["taps"]
+    passes = [(0, w), (1, w), (2, w)]
+    assert (O.compose(view, passes, O.WRAP, O.U8, O.STORE_ROUND) == d["round_once"]).all()
+    assert (O.compose(view, passes, O.WRAP, O.U8, O.STORE_CAST) == d["cast_each"]).all()
+    # the two modes really differ (truncate per pass vs round once)
+    assert (d["round_once"] != d["cast_each"]).mean() > 0.5
+
+
+def test_oracle_matches_golden_float_chains():
+    d, _ = golden("f32_rand9_reflect")
+    t = d["taps"]
+    passes = [(0, t[0]), (1, t[1]), (2, t[2])]
+    assert (O.compose(d["src"], passes, O.REFLECT, O.F32) == d["out"]).all()
+    assert (O.compose_total(d["src"], passes, O.REFLECT) == d["out_f64"]).all()
+    d, _ = golden("video4d_f32")
+    gx, gt = O.gaussian_weights(2.5), O.gaussian_weights(1.5)
+    passes = [(0, gx), (1, gx), (3, gt)]
+    assert (O.compose_total(d["src"], passes, O.REFLECT) == d["out_f64"]).all()
+
+
+def test_oracle_matches_golden_unit_and_1d():
+    d, _ = golden("unit_known_answers")
+    for b in (0, 1, 2):
+        assert (_i32(O.convolve_total(d["img"], np.ones((3, 3)), b)) == d["sum3_b%d" % b]).all()
+        assert (_i32(O.convolve_total(d["img"], np.ones((5, 5)), b)) == d["sum5_b%d" % b]).all()
+    assert (_i32(O.convolve_total(d["img54"], d["kb"], O.WRAP)) == d["composite_wrap"]).all()
+    assert (O.convolve_total(d["fimg"], d["fk"], O.WRAP) == d["fft_wrap"]).all()
+    d, _ = golden("one_d")
+    assert (O.cast(O.convolve_total(d["a"], d["box"]), O.F32) == d["out_box"]).all()
+    assert (O.gaussian_blur(d["x6"], 2.0, O.REFLECT) == d["out_g1"]).all()
+    d, _ = golden("u8_trunc_axis")
+    for ax in range(3):
+        assert (O.compose(d["src"], [(ax, d["taps"])], O.REFLECT, O.U8) == d["ax%d" % ax]).all()
+
+
+def test_adjoint_oracle_is_the_transpose():
+    """<P x, g> == <x, P^T g> for each border, and tap gradients equal the
+    finite-difference derivative (exact for a linear map)."""
+    rng = np.random.default_rng(5)
+    x = rng.standard_normal((7, 9, 11))
+    g = rng.standard_normal((7, 9, 11))
+    w = rng.standard_normal(5)
+    for b in (O.CLAMP, O.WRAP, O.REFLECT):
+        for ax in range(3):
+            lhs = (O.axis_pass_total(x, ax, w, b) * g).sum()
+            rhs = (x * O.axis_pass_adjoint(g, ax, w, b)).sum()
+            assert abs(lhs - rhs) < 1e-9 * (abs(lhs) + 1)
+            tg = O.axis_tap_grad(g, x, ax, len(w), b)
+            for k in range(len(w)):
+                e = np.zeros_like(w)
+                e[k] = 1.0
+                assert abs(tg[k] - (O.axis_pass_total(x, ax, e, b) * g).sum()) < 1e-9 * (abs(tg[k]) + 1)
+
+
+@pytest.mark.skipif(not O.have_reference(), reason="compiled reference not present")
+@pytest.mark.parametrize("seed", range(6))
+def test_oracle_matches_compiled_reference_random(seed):
+    rng = np.random.default_rng(seed)
+    shape = tuple(int(v) for v in rng.integers(3, 12, size=int(rng.integers(1, 4))))
+    b = int(rng.integers(0, 3))
+    for dt in (np.uint8, np.int16, np.float32, np.float64):
+        if np.issubdtype(dt, np.integer):
+            x = rng.integers(0, 100, shape).astype(dt)
+        else:
+            x = rng.standard_normal(shape).astype(dt)
+        kshape = tuple(int(v) for v in rng.integers(1, min(shape) + 1, size=len(shape)))
+        k = rng.standard_normal(kshape)
+        k[rng.random(kshape) < 0.2] = 0.0
+        ref = O.ref_convolve(x, k, b)
+        ours = O.cast(O.convolve_total(x, k, b), O.dtype_code(x))
+        assert (ref == ours).all() or (np.isnan(ref) == np.isnan(ours)).all()
+        sig = float(rng.uniform(0.4, 1.2))
+        if b == O.CLAMP or 2 * O.gaussian_radius(sig) < min(shape):
+            assert (O.ref_gaussian_blur(x, sig, b) == O.gaussian_blur(x, sig, b)).all()
