@@ -1,0 +1,457 @@
+"""Benchmark: 3-D separable convolution forward + adjoint on B200.
+
+One step = the forward chain Y = Cz(Cy(Cx X)) and its adjoint (dL/dX and all
+27 tap gradients of L = sum(W * Y)) over a batch of 192^3 float32 volumes:
+per-axis 9-tap kernels (N(0,1) taps, each normalised to unit L1 norm),
+border Reflect, X and W ~ N(0,1) from a seed.  The batch (8 volumes, an
+untouched fourth axis) makes the inputs 226 MB each -- larger than the 126 MB
+L2 -- so every step streams from HBM.
+
+Printed on rank 0: one JSON line with the headline throughput (Gvoxel/s of
+fwd+adjoint), the roofline of the dominant kernel, the end-to-end number
+through the C ABI with host buffers, the CPU baseline (the compiled ndl
+reference, single-threaded) and the other forms (uint8 bit-exact volume,
+bf16/f16/f32 video, 2-D gaussian, the batched uneven launch).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Gvoxel/s & % HBM peak, 3-D separable conv fwd+adjoint, FP32 plain vs batched BF16"
+EDGE, NTAP, BATCH = 192, 9, 8
+SEED = 20261203
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def make_taps(seed=SEED):
+    rng = np.random.default_rng(seed)
+    out = []
+    for ax in range(3):
+        w = rng.standard_normal(NTAP)
+        out.append((ax, w / np.abs(w).sum()))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region (NVML sampler thread)
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    REASONS = {
+        0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
+        0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown",
+    }
+
+    def __init__(self, index):
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self._stop = threading.Event()
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.nv = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            self.sample()
+            time.sleep(0.02)
+
+    def sample(self):
+        if self.nv is None:
+            return
+        try:
+            self.samples.append(self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+            mask = self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+            for bit, name in self.REASONS.items():
+                if mask & bit and name != "gpu_idle":
+                    self.reasons.add(name)
+        except Exception:
+            pass
+
+    def __enter__(self):
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self.t.join()
+        if not self.samples:
+            self.sample()
+
+    def result(self):
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None,
+                "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+
+def run_gpu(args):
+    import torch
+    import torch.distributed as dist
+
+    import ndl_b200 as n
+    from ndl_b200 import BorderMode, Image, abi
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local if world > 1 else 0)
+    torch.cuda.set_device(dev)
+    lib = abi.load()
+    hbm, peak_src = peaks()
+    passes = make_taps()
+    stream = torch.cuda.current_stream()
+
+    # workload: BATCH volumes of EDGE^3 (numpy shape (B, z, y, x))
+    g = torch.Generator(device=dev)
+    g.manual_seed(SEED + rank)
+    shape = (BATCH, EDGE, EDGE, EDGE)
+    X = torch.randn(shape, generator=g, device=dev, dtype=torch.float32)
+    W = torch.randn(shape, generator=g, device=dev, dtype=torch.float32)
+    Y = torch.empty_like(X)
+    GX = torch.empty_like(X)
+    taps = torch.zeros(3 * NTAP, dtype=torch.float32, device=dev)
+    xi, wi, yi, gi = (Image.from_tensor(t) for t in (X, W, Y, GX))
+    ws_f = n.convolve_axes_workspace_size(xi, yi, passes, BorderMode.Reflect)
+    ws = torch.empty(max(1, ws_f), dtype=torch.uint8, device=dev)
+    import ctypes
+    arr, keep = abi.make_passes(passes)
+    gv, xv, gxv = wi.abi_view(), xi.abi_view(), gi.abi_view()
+    nb = ctypes.c_size_t(0)
+    abi.check(lib.ndlgpu_convolve_axes_adjoint_workspace_size(ctypes.byref(gv), ctypes.byref(xv), ctypes.byref(gxv),
+                                                              3, arr, BorderMode.Reflect, abi.F32, ctypes.byref(nb)))
+    wsa = torch.empty(max(1, nb.value), dtype=torch.uint8, device=dev)
+
+    def fwd():
+        n.convolve_axes(xi, yi, passes, BorderMode.Reflect, workspace=ws, stream=stream)
+
+    def adj():
+        n.convolve_axes_adjoint(wi, xi, gi, passes, BorderMode.Reflect, taps, workspace=wsa, stream=stream)
+
+    voxels = BATCH * EDGE ** 3
+    K, Wm = args.steps, max(3, args.warmup)
+    for _ in range(Wm):
+        if args.only != "adj":
+            fwd()
+        if args.only != "fwd":
+            adj()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    l0 = lib.ndlgpu_kernel_launches()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(dev.index)
+    with sampler:
+        t_start = torch.cuda.Event(enable_timing=True)
+        t_end = torch.cuda.Event(enable_timing=True)
+        t_start.record(stream)
+        for k in range(K):
+            ev[k][0].record(stream)
+            if args.only != "adj":
+                fwd()
+            ev[k][1].record(stream)
+            if args.only != "fwd":
+                adj()
+            ev[k][2].record(stream)
+        t_end.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    launches = lib.ndlgpu_kernel_launches() - l0
+    total_ms = t_start.elapsed_time(t_end)
+    fwd_ms = sum(e[0].elapsed_time(e[1]) for e in ev) / K
+    adj_ms = sum(e[1].elapsed_time(e[2]) for e in ev) / K
+    fwd_ms, adj_ms = max(fwd_ms, 1e-9), max(adj_ms, 1e-9)
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_step = total_ms / K
+    value = world * voxels / (ms_step * 1e-3) / 1e9
+
+    # roofline of the dominant call (forward: 8 B/voxel; adjoint with tap
+    # gradients: 12 B/voxel, both algorithmic)
+    fwd_gbs = 8.0 * voxels / (fwd_ms * 1e-3) / 1e9
+    adj_gbs = 12.0 * voxels / (adj_ms * 1e-3) / 1e9
+    if adj_ms >= fwd_ms:
+        dom = {"kernel": "adjoint (dL/dX + 27 tap gradients)", "bytes_per_voxel": 12, "ms": adj_ms, "gbs": adj_gbs}
+    else:
+        dom = {"kernel": "fused forward k_fused<9,9,9>", "bytes_per_voxel": 8, "ms": fwd_ms, "gbs": fwd_gbs}
+    roofline = {"bound": "hbm", "achieved": round(dom["gbs"], 1), "peak": hbm, "unit": "GB/s",
+                "frac": round(dom["gbs"] / hbm, 4), "traffic": None, "kernel": dom["kernel"],
+                "peak_source": peak_src, "traffic_note": "see profiles/ (ncu dram__bytes per launch)"}
+
+    # end to end through the C ABI with host (pinned) buffers
+    e2e = None
+    if not args.skip_e2e:
+        hX = torch.empty(shape, dtype=torch.float32, pin_memory=True)
+        hW = torch.empty(shape, dtype=torch.float32, pin_memory=True)
+        hX.copy_(X)
+        hW.copy_(W)
+        hY = torch.empty_like(hX, pin_memory=True)
+        hG = torch.empty_like(hX, pin_memory=True)
+        htaps = torch.empty(3 * NTAP, dtype=torch.float32, pin_memory=True)
+        ke = max(3, min(K, 10))
+
+        def e2e_step():
+            X.copy_(hX, non_blocking=True)
+            W.copy_(hW, non_blocking=True)
+            fwd()
+            adj()
+            hY.copy_(Y, non_blocking=True)
+            hG.copy_(GX, non_blocking=True)
+            htaps.copy_(taps, non_blocking=True)
+
+        for _ in range(2):
+            e2e_step()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(ke):
+            e2e_step()
+        b.record(stream)
+        torch.cuda.synchronize()
+        ems = a.elapsed_time(b) / ke
+        if world > 1:
+            t = torch.tensor([ems], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": round(world * voxels / (ems * 1e-3) / 1e9, 3), "unit": "Gvoxel/s",
+               "h2d_bytes_per_step": 2 * X.numel() * 4, "d2h_bytes_per_step": 2 * X.numel() * 4 + 3 * NTAP * 4,
+               "ms_per_step": round(ems, 3)}
+
+    forms = {}
+    if rank == 0 and not args.skip_forms:
+        forms = other_forms(args, hbm)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        cpu = cpu_baseline_sample()
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "Gvoxel/s", "n_gpus": world, "steps": K, "warmup": Wm,
+        "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded N(0,1) volumes and taps)",
+        "config": {"workload": "config 3: %d volumes of %d^3 f32 per step, per-axis 9-tap L1-normalised N(0,1) "
+                               "kernels, Reflect; forward + adjoint (dL/dX and 27 tap gradients of sum(W*Y))"
+                               % (BATCH, EDGE),
+                   "voxels_per_step": voxels, "l2": "inputs larger than L2 (226 MB per tensor)",
+                   "parallelism": "replicas%d" % world},
+        "forward": {"ms": round(fwd_ms, 4), "gvoxel_s": round(voxels / fwd_ms / 1e6, 2),
+                    "gbs": round(fwd_gbs, 1), "frac_of_measured_hbm": round(fwd_gbs / hbm, 4)},
+        "adjoint": {"ms": round(adj_ms, 4), "gvoxel_s": round(voxels / adj_ms / 1e6, 2),
+                    "gbs": round(adj_gbs, 1), "frac_of_measured_hbm": round(adj_gbs / hbm, 4)},
+        "roofline": roofline, "e2e": e2e, "gpu_launches": int(launches), "clocks": sampler.result(),
+        "cpu_baseline": cpu, "forms": forms,
+    }
+    print(json.dumps(line))
+
+
+def time_call(fn, iters, warm=3):
+    import torch
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(iters):
+        fn()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / iters
+
+
+def other_forms(args, hbm):
+    """The other BASELINE configurations, timed briefly (each > L2)."""
+    import torch
+
+    import ndl_b200 as n
+    from ndl_b200 import BorderMode, Image
+
+    out = {}
+    it = max(5, min(args.steps, 20))
+    # config 2: uint8 256^3 through swap_axes(0,2).mirror(1), binomial, Wrap (x4 volumes > L2)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(SEED)
+    base = torch.randint(0, 256, (4, 256, 256, 256), generator=g, device="cuda", dtype=torch.uint8)
+    src = Image.from_tensor(base).swap_axes(0, 2).mirror(1)
+    dst = Image.empty(src.extent(), torch.uint8)
+    w = [1 / 16, 4 / 16, 6 / 16, 4 / 16, 1 / 16]
+    passes = [(0, w), (1, w), (2, w)]
+    ms = time_call(lambda: n.convolve_axes(src, dst, passes, BorderMode.Wrap), it)
+    vox = base.numel()
+    out["u8_binomial_256^3_view_x4"] = {"ms": round(ms, 4), "gvoxel_s": round(vox / ms / 1e6, 2),
+                                        "gbs": round(2.0 * vox / ms / 1e6, 1),
+                                        "frac_of_measured_hbm": round(2.0 * vox / ms / 1e6 / hbm, 4),
+                                        "exact": "bit-exact integer path"}
+    del base, src, dst
+    # config 5: 4-D video 1024x1024x3x96, sigma (2.5, 2.5, -, 1.5), Reflect
+    for name, dt in (("video_bf16", torch.bfloat16), ("video_f16", torch.float16), ("video_f32", torch.float32)):
+        v = torch.rand((96, 3, 1024, 1024), generator=g, device="cuda", dtype=torch.float32)
+        salt = torch.rand(v.shape, generator=g, device="cuda") < 0.01
+        v[salt] = 1.0
+        v = v.to(dt)
+        s = Image.from_tensor(v)
+        o = Image.empty(s.extent(), dt)
+        ms = time_call(lambda: n.gaussian_blur_axes(s, o, [2.5, 2.5, 0.0, 1.5], BorderMode.Reflect), max(3, it // 4))
+        vox = v.numel()
+        es = v.element_size()
+        out[name] = {"ms": round(ms, 3), "gvoxel_s": round(vox / ms / 1e6, 2), "gbs": round(2.0 * es * vox / ms / 1e6, 1),
+                     "frac_of_measured_hbm": round(2.0 * es * vox / ms / 1e6 / hbm, 4)}
+        del v, s, o, salt
+    # config 1: 2-D 512^2 gaussian sigma 2 (L2-resident; launch-bound)
+    im = torch.rand((512, 512), generator=g, device="cuda")
+    s = Image.from_tensor(im)
+    o = Image.empty(s.extent(), torch.float32)
+    ms = time_call(lambda: n.gaussian_blur(s, o, 2.0, BorderMode.Clamp), 50)
+    out["gauss2d_512_f32"] = {"ms": round(ms, 4), "gvoxel_s": round(im.numel() / ms / 1e6, 3),
+                              "note": "2 MB, L2-resident and launch-bound"}
+    torch.cuda.empty_cache()
+    return out
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the compiled ndl reference (forward) and the FP64 port (the
+# reference has no adjoint)
+# ---------------------------------------------------------------------------
+
+def _cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
+def cpu_sample(depth, seed=SEED):
+    """One bounded sample: a 192 x 192 x depth f32 volume, forward through
+    the reference (or the port when the reference is absent) + FP64 port
+    adjoint.  Returns (voxels, seconds, kind)."""
+    from oracle import oracle as O
+    rng = np.random.default_rng(seed)
+    x = rng.standard_normal((depth, EDGE, EDGE)).astype(np.float32)
+    wv = rng.standard_normal((depth, EDGE, EDGE)).astype(np.float32)
+    passes = make_taps()
+    t0 = time.perf_counter()
+    if O.have_reference():
+        O.ref_compose(x, passes, O.REFLECT, np.float32)
+        kind = "reference"
+    else:
+        O.compose(x, passes, O.REFLECT, O.F32)
+        kind = "port"
+    O.compose_adjoint(wv, x, passes, O.REFLECT)
+    return x.size, time.perf_counter() - t0, kind
+
+
+def cpu_baseline_sample():
+    depth = 64
+    vox, sec, kind = cpu_sample(depth)
+    return {"value": round(vox / sec / 1e9, 6), "unit": "Gvoxel/s", "cores": 1, "kind": kind,
+            "sample": "one 192x192x%d f32 volume (1/8 of a 192^3 volume), single thread: forward = ndl convolve() "
+                      "x3 (compiled reference, -O3) + adjoint = FP64 oracle port (ndl has no adjoint); %.2f s; %s"
+                      % (depth, sec, _cpu_model())}
+
+
+def run_reference(args):
+    """--impl reference: the reference's own CPU path on all host threads
+    (independent samples in parallel; ndl's convolve() is single-threaded and
+    re-entrant, processing/convolution.h:64-70)."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from concurrent.futures import ThreadPoolExecutor
+    cores = os.cpu_count() or 1
+    depth = 8
+    K, Wm = args.steps, max(3, args.warmup)
+
+    def step():
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(cores) as ex:
+            res = list(ex.map(lambda i: cpu_sample(depth, SEED + i), range(cores)))
+        dt = time.perf_counter() - t0
+        return sum(r[0] for r in res), dt, res[0][2]
+
+    for _ in range(Wm):
+        step()
+    vox, sec, kind = 0, 0.0, "reference"
+    for _ in range(K):
+        v, s, kind = step()
+        vox += v
+        sec += s
+    value = vox / sec / 1e9
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 6), "unit": "Gvoxel/s", "n_gpus": world,
+            "steps": K, "warmup": Wm, "ms_per_step": round(1e3 * sec / K, 2), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "config 3 per-voxel work (192x192 planes, 9-tap x3, Reflect, fwd+adjoint)"},
+            "cpu_baseline": {"value": round(value, 6), "unit": "Gvoxel/s", "cores": cores, "kind": kind,
+                             "sample": "%d threads, each a 192x192x%d f32 volume per step: forward = ndl convolve() x3 "
+                                       "(compiled reference) + adjoint = FP64 oracle port; %s"
+                                       % (cores, depth, _cpu_model())},
+            "e2e": {"value": round(value, 6), "unit": "Gvoxel/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ndlgpu", choices=["ndlgpu", "reference"])
+    ap.add_argument("--skip-forms", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--only", default="", choices=["", "fwd", "adj"],
+                    help="time only one half of the step (for profiling captures)")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -190,6 +190,11 @@ NDLGPU_API ndlgpu_status ndlgpu_convolve_axes_adjoint_workspace_size(const ndlgp
                                                           int npass, const ndlgpu_axis_kernel* passes,
                                                           int border, int grad_taps_dtype, size_t* bytes);
 
+/* ---- instrumentation ---------------------------------------------------- */
+/* Number of CUDA kernels this library has launched in this process (all
+ * devices, all threads); no reference counterpart. */
+NDLGPU_API uint64_t ndlgpu_kernel_launches(void);
+
 /* ---- device guard word -------------------------------------------------- */
 /* Reads (and clears) the library's device-side guard word on the current
  * device after synchronising `stream`: 0 if no kernel guard fired. */

@@ -96,6 +96,7 @@ SIGNATURES = {
     "ndlgpu_convolve_axes_adjoint": (_I, [_PV, _PV, _PV, _I, _PK, _I, _VP, _I, _VP, _SZ, _VP]),
     "ndlgpu_convolve_axes_adjoint_workspace_size": (_I, [_PV, _PV, _PV, _I, _PK, _I, _I, ctypes.POINTER(_SZ)]),
     "ndlgpu_device_status": (_I, [_VP, ctypes.POINTER(ctypes.c_int32)]),
+    "ndlgpu_kernel_launches": (ctypes.c_uint64, []),
 }
 
 _lib = None

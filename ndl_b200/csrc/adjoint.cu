@@ -162,6 +162,7 @@ cudaError_t launch_pass_adjoint(Acc acc, const GenericPassParams& p, cudaStream_
     const unsigned g = grid_cap(p.total, 8);
     if (acc == Acc::F64) k_pass_adjoint<double><<<g, 256, 0, s>>>(p);
     else k_pass_adjoint<float><<<g, 256, 0, s>>>(p);
+    count_launch();
     return cudaGetLastError();
 }
 
@@ -176,6 +177,7 @@ cudaError_t launch_tap_grad(Acc acc, const TapGradParams& p, unsigned nblocks, v
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     k_tap_grad_final<<<(p.ntap + 127) / 128, 128, 0, s>>>(p.partial, (int)nblocks, p.ntap, out, out_dtype);
+    count_launch(2);
     return cudaGetLastError();
 }
 

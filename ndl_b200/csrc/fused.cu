@@ -239,6 +239,7 @@ cudaError_t launch_one(const FusedParams& p, cudaStream_t s)
     const int gz = (p.nz + p.zchunk - 1) / p.zchunk;
     if (gx > 0x7fffffffLL || gz > 65535) return cudaErrorInvalidConfiguration;
     k_fused<Tin, Tout, A, KX, KY, KZ><<<dim3((unsigned)gx, (unsigned)gz), NT, 0, s>>>(p);
+    count_launch();
     return cudaGetLastError();
 }
 

@@ -1,0 +1,388 @@
+// fused2.cu -- fused separable forward for float storage (f32 / bf16 / f16
+// in, FP32 accumulation): up to three 1-D passes, one HBM read and one write
+// per element.
+//
+// A CTA owns a TX x TY column tile of one batch item and streams a chunk of Z
+// planes (2.5-D blocking):
+//   load  : plane zi (border-mapped along Z) with its X/Y halos goes to a
+//           3-stage shared-memory ring by cp.async, two planes ahead of the
+//           compute.  Rows are border-mapped as whole rows; the columns that
+//           fall outside [0, nx) and ragged 16-byte chunks are copied element
+//           by element from their border-mapped column.
+//   X pass: shared-memory rows, 4 outputs per thread-unit from a register
+//           window (taps as compile-time offsets).
+//   Y pass: 4 columns x 2 rows of outputs per thread.
+//   Z pass: a KZ-deep register queue per thread; the slot of the newest plane
+//           rotates, and the queue is read through a compile-time slot
+//           dispatch so that no value is ever moved.
+// Border maps are Clamp / Wrap / Reflect of mathHelpers.h:23-25, applied to
+// load coordinates only.
+#include <utility>
+
+#include "dtype.cuh"
+
+namespace ndlgpu {
+
+namespace {
+
+constexpr int TX = 64;
+constexpr int STAGES = 3;
+
+template <class T> __device__ __forceinline__ float to_f(T v);
+template <> __device__ __forceinline__ float to_f<float>(float v) { return v; }
+template <> __device__ __forceinline__ float to_f<__nv_bfloat16>(__nv_bfloat16 v) { return __bfloat162float(v); }
+template <> __device__ __forceinline__ float to_f<__half>(__half v) { return __half2float(v); }
+
+template <class T> __device__ __forceinline__ T from_f(float v);
+template <> __device__ __forceinline__ float from_f<float>(float v) { return v; }
+template <> __device__ __forceinline__ __nv_bfloat16 from_f<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
+template <> __device__ __forceinline__ __half from_f<__half>(float v) { return __float2half_rn(v); }
+
+// 4 consecutive shared-memory elements (aligned to 4 elements) as floats.
+__device__ __forceinline__ void lds4(const float* p, float* v)
+{
+    const float4 t = *reinterpret_cast<const float4*>(p);
+    v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+}
+__device__ __forceinline__ void lds4(const __nv_bfloat16* p, float* v)
+{
+    const uint2 t = *reinterpret_cast<const uint2*>(p);
+    v[0] = __uint_as_float(t.x << 16); v[1] = __uint_as_float(t.x & 0xffff0000u);
+    v[2] = __uint_as_float(t.y << 16); v[3] = __uint_as_float(t.y & 0xffff0000u);
+}
+__device__ __forceinline__ void lds4(const __half* p, float* v)
+{
+    const uint2 t = *reinterpret_cast<const uint2*>(p);
+    const __half2 a = *reinterpret_cast<const __half2*>(&t.x);
+    const __half2 b = *reinterpret_cast<const __half2*>(&t.y);
+    const float2 fa = __half22float2(a), fb = __half22float2(b);
+    v[0] = fa.x; v[1] = fa.y; v[2] = fb.x; v[3] = fb.y;
+}
+
+// 4 consecutive outputs to global memory (aligned when vec is set).
+__device__ __forceinline__ void stg4(float* p, const float* v) { *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]); }
+__device__ __forceinline__ void stg4(__nv_bfloat16* p, const float* v)
+{
+    __nv_bfloat162 a = __floats2bfloat162_rn(v[0], v[1]), b = __floats2bfloat162_rn(v[2], v[3]);
+    uint2 t;
+    t.x = *reinterpret_cast<uint32_t*>(&a);
+    t.y = *reinterpret_cast<uint32_t*>(&b);
+    *reinterpret_cast<uint2*>(p) = t;
+}
+__device__ __forceinline__ void stg4(__half* p, const float* v)
+{
+    __half2 a = __floats2half2_rn(v[0], v[1]), b = __floats2half2_rn(v[2], v[3]);
+    uint2 t;
+    t.x = *reinterpret_cast<uint32_t*>(&a);
+    t.y = *reinterpret_cast<uint32_t*>(&b);
+    *reinterpret_cast<uint2*>(p) = t;
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+template <class Tin, int KX, int KY, int TY_>
+struct Geo {
+    static constexpr int TY = TY_;
+    static constexpr int NT = 8 * TY;                           // 16 column groups x TY/2 row pairs
+    static constexpr int EPC = 16 / (int)sizeof(Tin);          // elements per 16-byte chunk
+    static constexpr int CX = KX / 2;
+    static constexpr int CY = KY / 2;
+    static constexpr int D = (EPC - CX % EPC) % EPC;          // smem column of global x0 - CX
+    static constexpr int ROWS = TY + KY - 1;
+    static constexpr int NCH = (TX + KX - 1 + D + EPC - 1) / EPC;
+    static constexpr int NV = (D % 4 + KX + 3 + 3) / 4;        // 4-wide loads per X window
+    static constexpr int WBASE = (D / 4) * 4;                   // first loaded column of a window
+    static constexpr int WOFF = D % 4;                          // window offset inside it
+    // elements per shared row: the loaded chunks, and every column an X
+    // window reads (the last window may read past the loaded chunks)
+    static constexpr int WEND = 60 + WBASE + 4 * NV;
+    static constexpr int PITCH = (NCH * EPC > WEND ? NCH * EPC : (WEND + EPC - 1) / EPC * EPC);
+    static constexpr int NTASK = (ROWS * NCH + NT - 1) / NT;
+    static constexpr int NXU = (ROWS * 16 + NT - 1) / NT;       // X-pass units per thread
+    static constexpr size_t IN_BYTES = (size_t)STAGES * ROWS * PITCH * sizeof(Tin);
+    static constexpr size_t X_BYTES = (size_t)ROWS * TX * sizeof(float);
+    // element-copy table: border columns and ragged chunks, built once per CTA
+    static constexpr int MAXEL = ROWS * PITCH;
+    static constexpr size_t TAB_BYTES = (size_t)MAXEL * 8;
+    static constexpr size_t SMEM = IN_BYTES + X_BYTES + TAB_BYTES + 16;
+};
+
+// Output plane sum of the Z queue for the newest slot S: tap k reads slot
+// (S + 1 + k) mod KZ (the queue holds the last KZ planes in ring order).
+template <int KZ, int S>
+__device__ __forceinline__ void zstep(float (&q)[KZ][8], const float (&yv)[8], float (&out)[8], const FusedParams& p)
+{
+#pragma unroll
+    for (int e = 0; e < 8; e++) q[S][e] = yv[e];
+#pragma unroll
+    for (int e = 0; e < 8; e++) {
+        float a = 0.f;
+#pragma unroll
+        for (int k = 0; k < KZ; k++) a = fmaf(q[(S + 1 + k) % KZ][e], p.wzf[k], a);
+        out[e] = a;
+    }
+}
+
+template <int KZ>
+__device__ __forceinline__ void zdispatch(int slot, float (&q)[KZ][8], const float (&yv)[8], float (&out)[8],
+                                          const FusedParams& p)
+{
+#define NDLGPU_ZCASE(S) \
+    case S:             \
+        if constexpr (S < KZ) zstep<KZ, (S < KZ ? S : 0)>(q, yv, out, p); \
+        break;
+    switch (slot) {
+        NDLGPU_ZCASE(0) NDLGPU_ZCASE(1) NDLGPU_ZCASE(2) NDLGPU_ZCASE(3) NDLGPU_ZCASE(4) NDLGPU_ZCASE(5)
+        NDLGPU_ZCASE(6) NDLGPU_ZCASE(7) NDLGPU_ZCASE(8) NDLGPU_ZCASE(9) NDLGPU_ZCASE(10) NDLGPU_ZCASE(11)
+        NDLGPU_ZCASE(12) NDLGPU_ZCASE(13) NDLGPU_ZCASE(14) NDLGPU_ZCASE(15) NDLGPU_ZCASE(16) NDLGPU_ZCASE(17)
+        NDLGPU_ZCASE(18) NDLGPU_ZCASE(19) NDLGPU_ZCASE(20) NDLGPU_ZCASE(21) NDLGPU_ZCASE(22) NDLGPU_ZCASE(23)
+        NDLGPU_ZCASE(24) NDLGPU_ZCASE(25) NDLGPU_ZCASE(26) NDLGPU_ZCASE(27) NDLGPU_ZCASE(28) NDLGPU_ZCASE(29)
+        NDLGPU_ZCASE(30) NDLGPU_ZCASE(31) NDLGPU_ZCASE(32) NDLGPU_ZCASE(33) NDLGPU_ZCASE(34) NDLGPU_ZCASE(35)
+        NDLGPU_ZCASE(36)
+    default: break;
+    }
+#undef NDLGPU_ZCASE
+}
+
+template <class Tin, class Tout, int KX, int KY, int KZ, int TY>
+__global__ void __launch_bounds__(8 * TY, (TY <= 16 ? 4 : 2)) k_fused2(const __grid_constant__ FusedParams p)
+{
+    using G = Geo<Tin, KX, KY, TY>;
+    constexpr int NT = G::NT;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Tin* s_in = reinterpret_cast<Tin*>(smem_raw);
+    float* s_x = reinterpret_cast<float*>(smem_raw + G::IN_BYTES);
+    int2* s_tab = reinterpret_cast<int2*>(smem_raw + G::IN_BYTES + G::X_BYTES);
+    int* s_ntab = reinterpret_cast<int*>(smem_raw + G::IN_BYTES + G::X_BYTES + G::TAB_BYTES);
+
+    const int tid = threadIdx.x;
+    const int ntx = (p.nx + TX - 1) / TX;
+    const int nty = (p.ny + TY - 1) / TY;
+    const int tile = blockIdx.x % (ntx * nty);
+    const int bat = blockIdx.x / (ntx * nty);
+    const int x0 = (tile % ntx) * TX;
+    const int y0 = (tile / ntx) * TY;
+    const int zs = blockIdx.y * p.zchunk;
+    const int ze = min(p.nz, zs + p.zchunk);
+    if (zs >= ze) return;
+    const Tin* src = reinterpret_cast<const Tin*>(p.src) + (int64_t)bat * p.sb;
+    Tout* dst = reinterpret_cast<Tout*>(p.dst) + (int64_t)bat * p.db;
+
+    constexpr int CZ = KZ / 2;
+    constexpr int HZ = KZ - 1 - CZ;
+    const int gx0 = x0 - G::CX - G::D;    // global column of shared column 0 (multiple of EPC)
+
+    // Loader set-up, once per CTA.  Chunk t = tid + j*NT covers shared row
+    // r = t / NCH, columns [q*EPC, (q+1)*EPC).  A chunk lying inside [0, nx)
+    // on a 16-byte aligned row is one 16-byte copy (offsets kept in
+    // registers); every other element goes to a shared table of (shared
+    // offset, in-plane global offset) pairs with its column border-mapped.
+    if (tid == 0) *s_ntab = 0;
+    __syncthreads();
+    int32_t goff[G::NTASK];
+    int32_t soff[G::NTASK];
+#pragma unroll
+    for (int j = 0; j < G::NTASK; j++) {
+        const int t = tid + j * NT;
+        goff[j] = -1;
+        soff[j] = 0;
+        if (t >= G::ROWS * G::NCH) continue;
+        const int r = t / G::NCH;
+        const int q = t - r * G::NCH;
+        int y = y0 - G::CY + r;
+        y = (y >= p.ny + KY - 1 - G::CY) ? p.ny - 1 : map_border32(p.border, p.ny, y);
+        const int32_t rowoff = (int32_t)(y * p.sy);
+        const int cx0 = gx0 + q * G::EPC;
+        if (p.vec_ld && cx0 >= 0 && cx0 + G::EPC <= p.nx) {
+            goff[j] = rowoff + cx0;
+            soff[j] = r * G::PITCH + q * G::EPC;
+        } else {
+            for (int e = 0; e < G::EPC; e++) {
+                int x = cx0 + e;
+                x = (x >= p.nx + KX - 1 - G::CX || x < -G::CX) ? p.nx - 1 : map_border32(p.border, p.nx, x);
+                const int slot_i = atomicAdd(s_ntab, 1);
+                s_tab[slot_i] = make_int2(r * G::PITCH + q * G::EPC + e, rowoff + (int32_t)(x * p.sx));
+            }
+        }
+    }
+    __syncthreads();
+    const int ntab = *s_ntab;
+
+    auto issue = [&](int zi, int stage) {
+        const int zm = map_border32(p.border, p.nz, zi);
+        const Tin* pl = src + (int64_t)zm * p.sz;
+        Tin* sb = s_in + stage * (G::ROWS * G::PITCH);
+#pragma unroll
+        for (int j = 0; j < G::NTASK; j++)
+            if (goff[j] >= 0) cp_async16(sb + soff[j], pl + goff[j]);
+        for (int i = tid; i < ntab; i += NT) {
+            const int2 e = s_tab[i];
+            if constexpr (sizeof(Tin) == 4) cp_async4(sb + e.x, pl + e.y);
+            else sb[e.x] = pl[e.y];
+        }
+    };
+
+    const int zin0 = zs - CZ;
+    const int zin1 = ze - 1 + HZ;
+    const int nplanes = zin1 - zin0 + 1;
+#pragma unroll
+    for (int s = 0; s < STAGES - 1; s++) {
+        if (s < nplanes) issue(zin0 + s, s);
+        cp_async_commit();
+    }
+
+    const int gx = tid & 15;
+    const int gy = tid >> 4;
+    float q[KZ][8];
+#pragma unroll
+    for (int k = 0; k < KZ; k++)
+#pragma unroll
+        for (int e = 0; e < 8; e++) q[k][e] = 0.f;
+
+    int slot = 0;
+    for (int n = 0; n < nplanes; n++) {
+        cp_async_wait<STAGES - 2>();
+        __syncthreads();    // plane n visible; every thread is past the X pass of plane n-1
+        if (n + STAGES - 1 < nplanes) issue(zin0 + n + STAGES - 1, (n + STAGES - 1) % STAGES);
+        cp_async_commit();
+
+        const Tin* sb = s_in + (n % STAGES) * (G::ROWS * G::PITCH);
+        // X pass: ROWS x 16 units of 4 outputs
+#pragma unroll
+        for (int i = 0; i < G::NXU; i++) {
+            const int u = tid + i * NT;
+            if (G::NXU * NT != G::ROWS * 16 && u >= G::ROWS * 16) break;
+            const int r = u >> 4, g = u & 15;
+            float win[G::NV * 4];
+#pragma unroll
+            for (int v = 0; v < G::NV; v++) lds4(sb + r * G::PITCH + 4 * g + G::WBASE + 4 * v, win + 4 * v);
+            float acc[4];
+#pragma unroll
+            for (int m = 0; m < 4; m++) {
+                float a = 0.f;
+#pragma unroll
+                for (int k = 0; k < KX; k++) a = fmaf(win[G::WOFF + m + k], p.wxf[k], a);
+                acc[m] = a;
+            }
+            *reinterpret_cast<float4*>(s_x + r * TX + 4 * g) = make_float4(acc[0], acc[1], acc[2], acc[3]);
+        }
+        __syncthreads();
+        // Y pass
+        float yv[8];
+#pragma unroll
+        for (int e = 0; e < 8; e++) yv[e] = 0.f;
+#pragma unroll
+        for (int j = 0; j < KY + 1; j++) {
+            const float4 v = *reinterpret_cast<const float4*>(s_x + (2 * gy + j) * TX + 4 * gx);
+            if (j < KY) {
+                yv[0] = fmaf(v.x, p.wyf[j], yv[0]); yv[1] = fmaf(v.y, p.wyf[j], yv[1]);
+                yv[2] = fmaf(v.z, p.wyf[j], yv[2]); yv[3] = fmaf(v.w, p.wyf[j], yv[3]);
+            }
+            if (j >= 1) {
+                yv[4] = fmaf(v.x, p.wyf[j - 1], yv[4]); yv[5] = fmaf(v.y, p.wyf[j - 1], yv[5]);
+                yv[6] = fmaf(v.z, p.wyf[j - 1], yv[6]); yv[7] = fmaf(v.w, p.wyf[j - 1], yv[7]);
+            }
+        }
+        // Z pass
+        float out[8];
+        zdispatch<KZ>(slot, q, yv, out, p);
+        slot = (slot + 1 == KZ) ? 0 : slot + 1;
+        if (n >= KZ - 1) {
+            const int zo = zin0 + n - HZ;
+            const int xb = x0 + 4 * gx;
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int y = y0 + 2 * gy + h;
+                if (y >= p.ny) continue;
+                Tout* row = dst + (int64_t)zo * p.dz + (int64_t)y * p.dy;
+                if (p.vec_st && xb + 4 <= p.nx) {
+                    stg4(row + xb, out + 4 * h);
+                } else {
+#pragma unroll
+                    for (int m = 0; m < 4; m++)
+                        if (xb + m < p.nx) row[(int64_t)(xb + m) * p.dx] = from_f<Tout>(out[4 * h + m]);
+                }
+            }
+        }
+    }
+    cp_async_wait<0>();
+}
+
+using LaunchFn = cudaError_t (*)(const FusedParams&, cudaStream_t);
+
+template <class Tin, class Tout, int KX, int KY, int KZ, int TY>
+cudaError_t launch2(const FusedParams& p, cudaStream_t s)
+{
+    using G = Geo<Tin, KX, KY, TY>;
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(k_fused2<Tin, Tout, KX, KY, KZ, TY>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    const int ntx = (p.nx + TX - 1) / TX;
+    const int nty = (p.ny + TY - 1) / TY;
+    const long long gx = (long long)ntx * nty * p.nbatch;
+    // Z chunks: about one full wave of resident CTAs, chunks of >= 4*KZ planes
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long long slots = (long long)sms * (TY <= 16 ? 4 : 2);
+    long long chunks = (slots + gx - 1) / gx;
+    int zc = (int)((p.nz + chunks - 1) / chunks);
+    zc = max(zc, min(p.nz, 4 * KZ));
+    FusedParams pp = p;
+    pp.zchunk = max(1, zc);
+    const int gz = (p.nz + pp.zchunk - 1) / pp.zchunk;
+    if (gx > 0x7fffffffLL || gz > 65535) return cudaErrorInvalidConfiguration;
+    k_fused2<Tin, Tout, KX, KY, KZ, TY><<<dim3((unsigned)gx, (unsigned)gz), G::NT, G::SMEM, s>>>(pp);
+    count_launch();
+    return cudaGetLastError();
+}
+
+struct Variant2 {
+    int sdt, ddt, kx, ky, kz;
+    LaunchFn fn;
+};
+
+const Variant2 kVariants2[] = {
+    {NDLGPU_F32, NDLGPU_F32, 9, 9, 9, &launch2<float, float, 9, 9, 9, 16>},
+    {NDLGPU_F32, NDLGPU_F32, 13, 13, 1, &launch2<float, float, 13, 13, 1, 24>},
+    {NDLGPU_F32, NDLGPU_F32, 17, 17, 11, &launch2<float, float, 17, 17, 11, 16>},
+    {NDLGPU_BF16, NDLGPU_BF16, 17, 17, 11, &launch2<__nv_bfloat16, __nv_bfloat16, 17, 17, 11, 16>},
+    {NDLGPU_F16, NDLGPU_F16, 17, 17, 11, &launch2<__half, __half, 17, 17, 11, 16>},
+};
+
+}  // namespace
+
+bool fused2_supported(int sdt, int ddt, int kx, int ky, int kz)
+{
+    for (const Variant2& v : kVariants2)
+        if (v.sdt == sdt && v.ddt == ddt && v.kx == kx && v.ky == ky && v.kz == kz) return true;
+    return false;
+}
+
+cudaError_t launch_fused2(const FusedParams& p, cudaStream_t s)
+{
+    for (const Variant2& v : kVariants2)
+        if (v.sdt == p.src_dtype && v.ddt == p.dst_dtype && v.kx == p.kx && v.ky == p.ky && v.kz == p.kz) {
+            if (p.nx <= 0 || p.ny <= 0 || p.nz <= 0 || p.nbatch <= 0) return cudaSuccess;
+            return v.fn(p, s);
+        }
+    return cudaErrorNotSupported;
+}
+
+}  // namespace ndlgpu

@@ -157,6 +157,7 @@ cudaError_t launch_generic_pass(Acc acc, const GenericPassParams& p, cudaStream_
     case Acc::F32: k_generic_pass<float><<<g, 256, 0, s>>>(p); break;
     default: k_generic_pass<int32_t><<<g, 256, 0, s>>>(p); break;
     }
+    count_launch();
     return cudaGetLastError();
 }
 
@@ -166,6 +167,7 @@ cudaError_t launch_generic_nd(Acc acc, const GenericNdParams& p, cudaStream_t s)
     const unsigned g = grid_for(p.total);
     if (acc == Acc::F32) k_generic_nd<float><<<g, 256, 0, s>>>(p);
     else k_generic_nd<double><<<g, 256, 0, s>>>(p);
+    count_launch();
     return cudaGetLastError();
 }
 

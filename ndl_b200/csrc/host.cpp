@@ -5,6 +5,7 @@
 // call, so an error return means nothing was enqueued (the reference checks
 // with assert() only, processing/convolution.h:59,112 and image/core.h:557).
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -15,6 +16,9 @@
 namespace ndlgpu {
 
 static thread_local std::string t_last_error;
+static std::atomic<uint64_t> g_launches{0};
+
+void count_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 static ndlgpu_status fail(ndlgpu_status s, const std::string& msg)
 {
@@ -451,7 +455,8 @@ static bool plan_fused(const Canon& c, Acc acc, int compose, int border, FusedPa
     if (!dense(by_axis[0], &kx)) return false;
     if (role[1] >= 0 && !dense(by_axis[role[1]], &ky)) return false;
     if (role[2] >= 0 && !dense(by_axis[role[2]], &kz)) return false;
-    if (!fused_supported(acc, c.sdt, c.ddt, kx, ky, kz)) return false;
+    const bool v2 = (acc == Acc::F32) && fused2_supported(c.sdt, c.ddt, kx, ky, kz);
+    if (!v2 && !fused_supported(acc, c.sdt, c.ddt, kx, ky, kz)) return false;
 
     FusedParams& p = *fp;
     std::memset(&p, 0, sizeof(p));
@@ -504,6 +509,16 @@ static bool plan_fused(const Canon& c, Acc acc, int compose, int border, FusedPa
     fill(role[1] >= 0 ? by_axis[role[1]] : nullptr, ky, p.wyf, p.wyi, &shift);
     fill(role[2] >= 0 ? by_axis[role[2]] : nullptr, kz, p.wzf, p.wzi, &shift);
     p.shift = shift;
+    // 32-bit in-plane offsets in the kernels
+    const int ses = dtype_size(c.sdt), des = dtype_size(c.ddt);
+    if ((__int128)(p.ny - 1) * (p.sy < 0 ? -p.sy : p.sy) + (__int128)(p.nx - 1) * (p.sx < 0 ? -p.sx : p.sx) >= ((__int128)1 << 31))
+        return false;
+    // vector paths: 16-byte aligned source rows, 4-element aligned output rows
+    auto al = [](const void* ptr, int64_t bytes) { return ((uintptr_t)ptr % (uintptr_t)bytes) == 0; };
+    p.vec_ld = (p.sx == 1 && al(p.src, 16) && (p.sy * ses) % 16 == 0 && (p.sz * ses) % 16 == 0 &&
+                (p.sb * ses) % 16 == 0) ? 1 : 0;
+    p.vec_st = (p.dx == 1 && al(p.dst, 4 * des) && (p.dy % 4) == 0 && (p.dz % 4) == 0 && (p.db % 4) == 0) ? 1 : 0;
+    p.vec_st = v2 ? p.vec_st : 0;
     // Z chunk: enough CTAs for two waves over the SMs, chunks >= 4*KZ planes
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -541,7 +556,10 @@ static ndlgpu_status execute(const Canon& c, const Plan& pl, int compose, int bo
 {
     if (c.total == 0) return NDLGPU_OK;
     if (pl.fused) {
-        cudaError_t e = launch_fused(pl.acc, pl.fp, s);
+        cudaError_t e = (pl.acc == Acc::F32 && fused2_supported(pl.fp.src_dtype, pl.fp.dst_dtype, pl.fp.kx, pl.fp.ky,
+                                                                 pl.fp.kz))
+                            ? launch_fused2(pl.fp, s)
+                            : launch_fused(pl.acc, pl.fp, s);
         if (e != cudaSuccess) return cuda_fail(e, "fused kernel");
         return NDLGPU_OK;
     }
@@ -1152,6 +1170,8 @@ ndlgpu_status ndlgpu_convolve_axes_adjoint(const ndlgpu_view* grad_out, const nd
     return adjoint_execute(grad_out, src, grad_src, border, grad_taps, grad_taps_dtype, ap, workspace,
                            workspace_bytes, (cudaStream_t)stream);
 }
+
+uint64_t ndlgpu_kernel_launches(void) { return g_launches.load(std::memory_order_relaxed); }
 
 ndlgpu_status ndlgpu_device_status(void* stream, int32_t* code)
 {

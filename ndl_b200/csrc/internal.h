@@ -167,6 +167,8 @@ struct FusedParams {
     int cx, cy, cz;       // centre = -(offset of tap 0)
     int shift;            // Acc::I32 total shift
     int zchunk;           // output planes per CTA along Z
+    int vec_ld;           // source rows 16-byte aligned with sx == 1
+    int vec_st;           // destination rows 4-element aligned with dx == 1
     float wxf[64], wyf[64], wzf[64];
     int32_t wxi[64], wyi[64], wzi[64];
 };
@@ -174,6 +176,12 @@ struct FusedParams {
 // Returns cudaErrorNotSupported when no compiled variant matches.
 cudaError_t launch_fused(Acc acc, const FusedParams& p, cudaStream_t s);
 bool fused_supported(Acc acc, int src_dtype, int dst_dtype, int kx, int ky, int kz);
+// Float-storage fused kernel with asynchronous loads (fused2.cu).
+cudaError_t launch_fused2(const FusedParams& p, cudaStream_t s);
+bool fused2_supported(int src_dtype, int dst_dtype, int kx, int ky, int kz);
+
+// Process-wide count of kernel launches (ndlgpu_kernel_launches).
+void count_launch(unsigned n = 1);
 
 // Device guard word.
 cudaError_t read_device_status(cudaStream_t s, int32_t* code);
