@@ -190,6 +190,29 @@ NDLGPU_API ndlgpu_status ndlgpu_convolve_axes_adjoint_workspace_size(const ndlgp
                                                           int npass, const ndlgpu_axis_kernel* passes,
                                                           int border, int grad_taps_dtype, size_t* bytes);
 
+/* ---- allocation-free gaussian_blur ---------------------------------------
+ * No counterpart in the reference.  Some callers cannot allocate device
+ * memory: plugins hosted by an application that owns the GPU's memory pool
+ * and forbids allocations behind its back, real-time loops that must never
+ * reach the allocator (cudaMalloc can synchronise the device and takes an
+ * unbounded time), and code held to a static memory budget.  This entry point
+ * is ndlgpu_gaussian_blur with its scratch taken from a fixed device array
+ * inside libndlgpu.so, so it calls no allocating routine; the caller still
+ * passes src and dst.
+ *   - The array is NDLGPU_NOALLOC_SCRATCH_BYTES (16 MiB); every GPU that loads
+ *     the library holds it until the process exits.  A blur whose scratch
+ *     (ndlgpu_gaussian_blur_workspace_size) exceeds it returns
+ *     NDLGPU_ERR_WORKSPACE and enqueues nothing.
+ *   - The first call on a device looks up the array's device address with the
+ *     device current; make that first call before any stream capture.
+ *   - All calls share the one array: calls that overlap on the GPU (other
+ *     streams, other host threads) race.  The blur writes every scratch
+ *     element before reading it, so the array needs no clearing between
+ *     calls. */
+#define NDLGPU_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
+NDLGPU_API ndlgpu_status ndlgpu_gaussian_blur_noalloc(const ndlgpu_view* src, const ndlgpu_view* dst,
+                                                      double sigma, int border, void* stream);
+
 /* ---- instrumentation ---------------------------------------------------- */
 /* Number of CUDA kernels this library has launched in this process (all
  * devices, all threads); no reference counterpart. */

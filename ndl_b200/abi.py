@@ -97,6 +97,7 @@ SIGNATURES = {
     "ndlgpu_convolve_axes_adjoint_workspace_size": (_I, [_PV, _PV, _PV, _I, _PK, _I, _I, ctypes.POINTER(_SZ)]),
     "ndlgpu_device_status": (_I, [_VP, ctypes.POINTER(ctypes.c_int32)]),
     "ndlgpu_kernel_launches": (ctypes.c_uint64, []),
+    "ndlgpu_gaussian_blur_noalloc": (_I, [_PV, _PV, ctypes.c_double, _I, _VP]),
 }
 
 _lib = None

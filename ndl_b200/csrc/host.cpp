@@ -20,6 +20,12 @@ static std::atomic<uint64_t> g_launches{0};
 
 void count_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
+ndlgpu_status set_error(ndlgpu_status s, const std::string& msg)
+{
+    t_last_error = msg;
+    return s;
+}
+
 static ndlgpu_status fail(ndlgpu_status s, const std::string& msg)
 {
     t_last_error = msg;

@@ -180,6 +180,9 @@ bool fused_supported(Acc acc, int src_dtype, int dst_dtype, int kx, int ky, int 
 cudaError_t launch_fused2(const FusedParams& p, cudaStream_t s);
 bool fused2_supported(int src_dtype, int dst_dtype, int kx, int ky, int kz);
 
+// Sets the per-thread message ndlgpu_last_error() returns; returns s.
+ndlgpu_status set_error(ndlgpu_status s, const std::string& msg);
+
 // Process-wide count of kernel launches (ndlgpu_kernel_launches).
 void count_launch(unsigned n = 1);
 
