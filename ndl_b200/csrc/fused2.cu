@@ -122,7 +122,8 @@ struct Geo {
 // Output plane sum of the Z queue for the newest slot S: tap k reads slot
 // (S + 1 + k) mod KZ (the queue holds the last KZ planes in ring order).
 template <int KZ, int S>
-__device__ __forceinline__ void zstep(float (&q)[KZ][8], const float (&yv)[8], float (&out)[8], const FusedParams& p)
+__device__ __forceinline__ void zstep(float (&q)[KZ][8], const float (&yv)[8], float (&out)[8], const FusedParams& p,
+                                      int ez)
 {
 #pragma unroll
     for (int e = 0; e < 8; e++) q[S][e] = yv[e];
@@ -133,15 +134,33 @@ __device__ __forceinline__ void zstep(float (&q)[KZ][8], const float (&yv)[8], f
         for (int k = 0; k < KZ; k++) a = fmaf(q[(S + 1 + k) % KZ][e], p.wzf[k], a);
         out[e] = a;
     }
+    if (ez >= 0) {   // adjoint border plane: effective weights
+#pragma unroll
+        for (int e = 0; e < 8; e++) {
+            float a = 0.f;
+#pragma unroll
+            for (int k = 0; k < KZ; k++) a = fmaf(q[(S + 1 + k) % KZ][e], p.zz[ez][k], a);
+            out[e] = a;
+        }
+    }
+}
+
+// Row of the effective-weight table for position j of an axis of extent n
+// with zone radius r, or -1 outside the zones.
+__device__ __forceinline__ int zone_row(int j, int n, int r)
+{
+    if (j < r) return j;
+    if (j >= n - r) return r + (j - (n - r));
+    return -1;
 }
 
 template <int KZ>
 __device__ __forceinline__ void zdispatch(int slot, float (&q)[KZ][8], const float (&yv)[8], float (&out)[8],
-                                          const FusedParams& p)
+                                          const FusedParams& p, int ez)
 {
 #define NDLGPU_ZCASE(S) \
     case S:             \
-        if constexpr (S < KZ) zstep<KZ, (S < KZ ? S : 0)>(q, yv, out, p); \
+        if constexpr (S < KZ) zstep<KZ, (S < KZ ? S : 0)>(q, yv, out, p, ez); \
         break;
     switch (slot) {
         NDLGPU_ZCASE(0) NDLGPU_ZCASE(1) NDLGPU_ZCASE(2) NDLGPU_ZCASE(3) NDLGPU_ZCASE(4) NDLGPU_ZCASE(5)
@@ -156,7 +175,7 @@ __device__ __forceinline__ void zdispatch(int slot, float (&q)[KZ][8], const flo
 #undef NDLGPU_ZCASE
 }
 
-template <class Tin, class Tout, int KX, int KY, int KZ, int TY>
+template <class Tin, class Tout, int KX, int KY, int KZ, int TY, bool ADJ>
 __global__ void __launch_bounds__(8 * TY, (TY <= 16 ? 4 : 2)) k_fused2(const __grid_constant__ FusedParams p)
 {
     using G = Geo<Tin, KX, KY, TY>;
@@ -189,6 +208,7 @@ __global__ void __launch_bounds__(8 * TY, (TY <= 16 ? 4 : 2)) k_fused2(const __g
     // on a 16-byte aligned row is one 16-byte copy (offsets kept in
     // registers); every other element goes to a shared table of (shared
     // offset, in-plane global offset) pairs with its column border-mapped.
+    const bool zp = ADJ && p.zero_pad;   // adjoint, Clamp/Reflect: zero outside the image
     if (tid == 0) *s_ntab = 0;
     __syncthreads();
     int32_t goff[G::NTASK];
@@ -202,15 +222,25 @@ __global__ void __launch_bounds__(8 * TY, (TY <= 16 ? 4 : 2)) k_fused2(const __g
         const int r = t / G::NCH;
         const int q = t - r * G::NCH;
         int y = y0 - G::CY + r;
+        const int cx0 = gx0 + q * G::EPC;
+        if (zp && (y < 0 || y >= p.ny)) {
+            // a row outside the image: zero in every stage, never copied
+            for (int e = 0; e < G::EPC; e++)
+                for (int st = 0; st < STAGES; st++) s_in[st * (G::ROWS * G::PITCH) + r * G::PITCH + q * G::EPC + e] = Tin(0.f);
+            continue;
+        }
         y = (y >= p.ny + KY - 1 - G::CY) ? p.ny - 1 : map_border32(p.border, p.ny, y);
         const int32_t rowoff = (int32_t)(y * p.sy);
-        const int cx0 = gx0 + q * G::EPC;
         if (p.vec_ld && cx0 >= 0 && cx0 + G::EPC <= p.nx) {
             goff[j] = rowoff + cx0;
             soff[j] = r * G::PITCH + q * G::EPC;
         } else {
             for (int e = 0; e < G::EPC; e++) {
                 int x = cx0 + e;
+                if (zp && (x < 0 || x >= p.nx)) {
+                    for (int st = 0; st < STAGES; st++) s_in[st * (G::ROWS * G::PITCH) + r * G::PITCH + q * G::EPC + e] = Tin(0.f);
+                    continue;
+                }
                 x = (x >= p.nx + KX - 1 - G::CX || x < -G::CX) ? p.nx - 1 : map_border32(p.border, p.nx, x);
                 const int slot_i = atomicAdd(s_ntab, 1);
                 s_tab[slot_i] = make_int2(r * G::PITCH + q * G::EPC + e, rowoff + (int32_t)(x * p.sx));
@@ -221,9 +251,17 @@ __global__ void __launch_bounds__(8 * TY, (TY <= 16 ? 4 : 2)) k_fused2(const __g
     const int ntab = *s_ntab;
 
     auto issue = [&](int zi, int stage) {
+        Tin* sb = s_in + stage * (G::ROWS * G::PITCH);
+        if (zp && (zi < 0 || zi >= p.nz)) {
+            // a plane outside the image: zero what the copies would fill
+#pragma unroll
+            for (int j = 0; j < G::NTASK; j++)
+                if (goff[j] >= 0) *reinterpret_cast<uint4*>(sb + soff[j]) = make_uint4(0u, 0u, 0u, 0u);
+            for (int i = tid; i < ntab; i += NT) sb[s_tab[i].x] = Tin(0.f);
+            return;
+        }
         const int zm = map_border32(p.border, p.nz, zi);
         const Tin* pl = src + (int64_t)zm * p.sz;
-        Tin* sb = s_in + stage * (G::ROWS * G::PITCH);
 #pragma unroll
         for (int j = 0; j < G::NTASK; j++)
             if (goff[j] >= 0) cp_async16(sb + soff[j], pl + goff[j]);
@@ -276,6 +314,20 @@ __global__ void __launch_bounds__(8 * TY, (TY <= 16 ? 4 : 2)) k_fused2(const __g
                 for (int k = 0; k < KX; k++) a = fmaf(win[G::WOFF + m + k], p.wxf[k], a);
                 acc[m] = a;
             }
+            if (zp) {
+                const int xg0 = x0 + 4 * g;
+                if (xg0 < G::CX || xg0 + 3 >= p.nx - G::CX) {
+#pragma unroll
+                    for (int m = 0; m < 4; m++) {
+                        const int e = zone_row(xg0 + m, p.nx, G::CX);
+                        if (e < 0) continue;
+                        float a = 0.f;
+#pragma unroll
+                        for (int k = 0; k < KX; k++) a = fmaf(win[G::WOFF + m + k], p.zx[e][k], a);
+                        acc[m] = a;
+                    }
+                }
+            }
             *reinterpret_cast<float4*>(s_x + r * TX + 4 * g) = make_float4(acc[0], acc[1], acc[2], acc[3]);
         }
         __syncthreads();
@@ -295,9 +347,25 @@ __global__ void __launch_bounds__(8 * TY, (TY <= 16 ? 4 : 2)) k_fused2(const __g
                 yv[6] = fmaf(v.z, p.wyf[j - 1], yv[6]); yv[7] = fmaf(v.w, p.wyf[j - 1], yv[7]);
             }
         }
+        if (zp) {
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int e = zone_row(y0 + 2 * gy + h, p.ny, G::CY);
+                if (e < 0) continue;
+                float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+#pragma unroll
+                for (int j = 0; j < KY; j++) {
+                    const float4 v = *reinterpret_cast<const float4*>(s_x + (2 * gy + h + j) * TX + 4 * gx);
+                    const float w = p.zy[e][j];
+                    a0 = fmaf(v.x, w, a0); a1 = fmaf(v.y, w, a1); a2 = fmaf(v.z, w, a2); a3 = fmaf(v.w, w, a3);
+                }
+                yv[4 * h] = a0; yv[4 * h + 1] = a1; yv[4 * h + 2] = a2; yv[4 * h + 3] = a3;
+            }
+        }
         // Z pass
         float out[8];
-        zdispatch<KZ>(slot, q, yv, out, p);
+        const int ez = zp ? zone_row(zin0 + n - HZ, p.nz, CZ) : -1;
+        zdispatch<KZ>(slot, q, yv, out, p, ez);
         slot = (slot + 1 == KZ) ? 0 : slot + 1;
         if (n >= KZ - 1) {
             const int zo = zin0 + n - HZ;
@@ -322,13 +390,13 @@ __global__ void __launch_bounds__(8 * TY, (TY <= 16 ? 4 : 2)) k_fused2(const __g
 
 using LaunchFn = cudaError_t (*)(const FusedParams&, cudaStream_t);
 
-template <class Tin, class Tout, int KX, int KY, int KZ, int TY>
+template <class Tin, class Tout, int KX, int KY, int KZ, int TY, bool ADJ>
 cudaError_t launch2(const FusedParams& p, cudaStream_t s)
 {
     using G = Geo<Tin, KX, KY, TY>;
     static bool configured = false;
     if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(k_fused2<Tin, Tout, KX, KY, KZ, TY>,
+        cudaError_t e = cudaFuncSetAttribute(k_fused2<Tin, Tout, KX, KY, KZ, TY, ADJ>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM);
         if (e != cudaSuccess) return e;
         configured = true;
@@ -348,37 +416,46 @@ cudaError_t launch2(const FusedParams& p, cudaStream_t s)
     pp.zchunk = max(1, zc);
     const int gz = (p.nz + pp.zchunk - 1) / pp.zchunk;
     if (gx > 0x7fffffffLL || gz > 65535) return cudaErrorInvalidConfiguration;
-    k_fused2<Tin, Tout, KX, KY, KZ, TY><<<dim3((unsigned)gx, (unsigned)gz), G::NT, G::SMEM, s>>>(pp);
+    k_fused2<Tin, Tout, KX, KY, KZ, TY, ADJ><<<dim3((unsigned)gx, (unsigned)gz), G::NT, G::SMEM, s>>>(pp);
     count_launch();
     return cudaGetLastError();
 }
 
 struct Variant2 {
-    int sdt, ddt, kx, ky, kz;
+    int adj, sdt, ddt, kx, ky, kz;
     LaunchFn fn;
 };
 
+#define NDLGPU_V2(A, TI, TO, DI, DO, KX_, KY_, KZ_, TY_) \
+    {A, DI, DO, KX_, KY_, KZ_, &launch2<TI, TO, KX_, KY_, KZ_, TY_, (A != 0)>}
 const Variant2 kVariants2[] = {
-    {NDLGPU_F32, NDLGPU_F32, 9, 9, 9, &launch2<float, float, 9, 9, 9, 16>},
-    {NDLGPU_F32, NDLGPU_F32, 13, 13, 1, &launch2<float, float, 13, 13, 1, 24>},
-    {NDLGPU_F32, NDLGPU_F32, 17, 17, 11, &launch2<float, float, 17, 17, 11, 16>},
-    {NDLGPU_BF16, NDLGPU_BF16, 17, 17, 11, &launch2<__nv_bfloat16, __nv_bfloat16, 17, 17, 11, 16>},
-    {NDLGPU_F16, NDLGPU_F16, 17, 17, 11, &launch2<__half, __half, 17, 17, 11, 16>},
+    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 9, 9, 9, 16),
+    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 13, 13, 1, 24),
+    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 17, 17, 11, 16),
+    NDLGPU_V2(0, __nv_bfloat16, __nv_bfloat16, NDLGPU_BF16, NDLGPU_BF16, 17, 17, 11, 16),
+    NDLGPU_V2(0, __half, __half, NDLGPU_F16, NDLGPU_F16, 17, 17, 11, 16),
+    NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 9, 9, 9, 16),
+    NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 13, 13, 1, 24),
+    NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 17, 17, 11, 16),
+    NDLGPU_V2(1, __nv_bfloat16, __nv_bfloat16, NDLGPU_BF16, NDLGPU_BF16, 17, 17, 11, 16),
+    NDLGPU_V2(1, __half, __half, NDLGPU_F16, NDLGPU_F16, 17, 17, 11, 16),
 };
+#undef NDLGPU_V2
 
 }  // namespace
 
-bool fused2_supported(int sdt, int ddt, int kx, int ky, int kz)
+bool fused2_supported(int sdt, int ddt, int kx, int ky, int kz, int adj)
 {
     for (const Variant2& v : kVariants2)
-        if (v.sdt == sdt && v.ddt == ddt && v.kx == kx && v.ky == ky && v.kz == kz) return true;
+        if (v.adj == adj && v.sdt == sdt && v.ddt == ddt && v.kx == kx && v.ky == ky && v.kz == kz) return true;
     return false;
 }
 
 cudaError_t launch_fused2(const FusedParams& p, cudaStream_t s)
 {
     for (const Variant2& v : kVariants2)
-        if (v.sdt == p.src_dtype && v.ddt == p.dst_dtype && v.kx == p.kx && v.ky == p.ky && v.kz == p.kz) {
+        if (v.adj == (p.adj ? 1 : 0) && v.sdt == p.src_dtype && v.ddt == p.dst_dtype && v.kx == p.kx &&
+            v.ky == p.ky && v.kz == p.kz) {
             if (p.nx <= 0 || p.ny <= 0 || p.nz <= 0 || p.nbatch <= 0) return cudaSuccess;
             return v.fn(p, s);
         }

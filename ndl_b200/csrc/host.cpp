@@ -415,8 +415,41 @@ struct Plan {
     int scratch_dtype = 0;
 };
 
-// Fused-kernel eligibility and parameters.
-static bool plan_fused(const Canon& c, Acc acc, int compose, int border, FusedParams* fp)
+// Effective weights of a transposed 1-D pass at the positions within r = K/2
+// of either end of an axis of extent M: for position j, window entry m (the
+// zero-padded input at j - r + m) collects every tap w_k whose forward read
+// of that input lands on j after the border map (map(i + o_k) == j).  The
+// transposed pass elsewhere is the plain flipped correlation.
+static void zone_table(int64_t M, int border, const std::vector<std::pair<int, double>>& taps, int K,
+                       float (*tab)[17])
+{
+    const int r = K / 2;
+    for (int e = 0; e < 16; e++)
+        for (int m = 0; m < 17; m++) tab[e][m] = 0.f;
+    for (int e = 0; e < 2 * r && e < 16; e++) {
+        const int64_t j = (e < r) ? e : (M - r + (e - r));
+        if (j < 0 || j >= M) continue;
+        double acc[17] = {0};
+        for (int m = 0; m < K; m++) {
+            const int64_t i = j - r + m;
+            if (i < 0 || i >= M) continue;
+            for (const auto& t : taps) {
+                int64_t pos = i + t.first;
+                if (pos < 0 || pos >= M) {
+                    if (border == NDLGPU_WRAP) pos = pos < 0 ? pos + M : pos - M;
+                    else if (border == NDLGPU_REFLECT) pos = pos < 0 ? -pos - 1 : 2 * M - pos - 1;
+                    else pos = pos < 0 ? 0 : M - 1;
+                }
+                if (pos == j) acc[m] += t.second;
+            }
+        }
+        for (int m = 0; m < K; m++) tab[e][m] = (float)acc[m];
+    }
+}
+
+// Fused-kernel eligibility and parameters.  adj: the transposed chain (the
+// input gradient), run by the float fused kernel only.
+static bool plan_fused(const Canon& c, Acc acc, int compose, int border, FusedParams* fp, int adj = 0)
 {
     if (acc != Acc::F32 && acc != Acc::I32) return false;
     if (c.passes.empty() || c.passes.size() > 3) return false;
@@ -461,7 +494,8 @@ static bool plan_fused(const Canon& c, Acc acc, int compose, int border, FusedPa
     if (!dense(by_axis[0], &kx)) return false;
     if (role[1] >= 0 && !dense(by_axis[role[1]], &ky)) return false;
     if (role[2] >= 0 && !dense(by_axis[role[2]], &kz)) return false;
-    const bool v2 = (acc == Acc::F32) && fused2_supported(c.sdt, c.ddt, kx, ky, kz);
+    const bool v2 = (acc == Acc::F32) && fused2_supported(c.sdt, c.ddt, kx, ky, kz, adj);
+    if (adj && !v2) return false;
     if (!v2 && !fused_supported(acc, c.sdt, c.ddt, kx, ky, kz)) return false;
 
     FusedParams& p = *fp;
@@ -515,6 +549,31 @@ static bool plan_fused(const Canon& c, Acc acc, int compose, int border, FusedPa
     fill(role[1] >= 0 ? by_axis[role[1]] : nullptr, ky, p.wyf, p.wyi, &shift);
     fill(role[2] >= 0 ? by_axis[role[2]] : nullptr, kz, p.wzf, p.wzi, &shift);
     p.shift = shift;
+    if (adj) {
+        // transposed passes: flipped taps; Clamp/Reflect read zeros outside
+        // the image and fold the border through the zone tables
+        p.adj = 1;
+        p.zero_pad = (border != NDLGPU_WRAP) ? 1 : 0;
+        auto flip = [](float* w, int K) { std::reverse(w, w + K); };
+        flip(p.wxf, kx);
+        flip(p.wyf, ky);
+        flip(p.wzf, kz);
+        auto sorted = [&](const CPass* cp) {
+            std::vector<std::pair<int, double>> t;
+            if (cp)
+                for (size_t i = 0; i < cp->off.size(); i++) t.push_back({cp->off[i], cp->w[i]});
+            else
+                t.push_back({0, 1.0});
+            std::sort(t.begin(), t.end());
+            return t;
+        };
+        if (p.zero_pad) {
+            if (kx > 17 || ky > 17 || kz > 17) return false;
+            zone_table(p.nx, border, sorted(by_axis[0]), kx, p.zx);
+            zone_table(p.ny, border, sorted(role[1] >= 0 ? by_axis[role[1]] : nullptr), ky, p.zy);
+            zone_table(p.nz, border, sorted(role[2] >= 0 ? by_axis[role[2]] : nullptr), kz, p.zz);
+        }
+    }
     // 32-bit in-plane offsets in the kernels
     const int ses = dtype_size(c.sdt), des = dtype_size(c.ddt);
     if ((__int128)(p.ny - 1) * (p.sy < 0 ? -p.sy : p.sy) + (__int128)(p.nx - 1) * (p.sx < 0 ? -p.sx : p.sx) >= ((__int128)1 << 31))
@@ -827,11 +886,34 @@ static size_t adjoint_workspace(const AdjPlan& ap)
     return (size_t)(ap.nF + ap.nB) * ap.elem_bytes + align_up((size_t)ap.nblocks * ap.maxk * sizeof(double));
 }
 
+// Fused input gradient (float types, up to three dense odd-tap passes on
+// distinct axes): the transposed chain in one kernel.
+static bool plan_fused_adjoint(const ndlgpu_view* g, const ndlgpu_view* gx, int npass,
+                               const ndlgpu_axis_kernel* passes, int border, FusedParams* fp)
+{
+    if (!float_dtype(g->dtype) || !float_dtype(gx->dtype) || g->dtype == NDLGPU_F64 || gx->dtype == NDLGPU_F64)
+        return false;
+    std::vector<LPass> lp;
+    const std::string keep = t_last_error;
+    if (lpasses_from(npass, passes, &lp) != NDLGPU_OK) { t_last_error = keep; return false; }
+    for (auto& p : lp)
+        for (double w : p.taps)
+            if (w == 0.0) return false;    // every tap must be present in the fused tap window
+    Canon c;
+    if (canonicalise(g, gx, lp, border, &c) != NDLGPU_OK || c.total == 0) { t_last_error = keep; return false; }
+    return plan_fused(c, Acc::F32, NDLGPU_ROUND_ONCE, border, fp, 1);
+}
+
 static ndlgpu_status adjoint_execute(const ndlgpu_view* g, const ndlgpu_view* x, const ndlgpu_view* gx,
                                      int border, void* grad_taps, int tdt, const AdjPlan& ap, void* ws,
-                                     size_t ws_bytes, cudaStream_t s)
+                                     size_t ws_bytes, cudaStream_t s, const FusedParams* fused_gx = nullptr)
 {
     if (ap.total == 0) return NDLGPU_OK;
+    if (fused_gx && !grad_taps) {
+        cudaError_t e = launch_fused2(*fused_gx, s);
+        if (e != cudaSuccess) return cuda_fail(e, "fused adjoint");
+        return NDLGPU_OK;
+    }
     Scratch sc;
     ndlgpu_status st = get_scratch(adjoint_workspace(ap), ws, ws_bytes, s, &sc);
     if (st != NDLGPU_OK) return st;
@@ -1173,8 +1255,11 @@ ndlgpu_status ndlgpu_convolve_axes_adjoint(const ndlgpu_view* grad_out, const nd
     ndlgpu_status st = adjoint_prepare(grad_out, src, grad_src, npass, passes, border, grad_taps != nullptr,
                                        grad_taps_dtype, &ap);
     if (st != NDLGPU_OK) return st;
+    FusedParams fp;
+    const bool fused = grad_src && !grad_taps && ap.total > 0 &&
+                       plan_fused_adjoint(grad_out, grad_src, npass, passes, border, &fp);
     return adjoint_execute(grad_out, src, grad_src, border, grad_taps, grad_taps_dtype, ap, workspace,
-                           workspace_bytes, (cudaStream_t)stream);
+                           workspace_bytes, (cudaStream_t)stream, fused ? &fp : nullptr);
 }
 
 uint64_t ndlgpu_kernel_launches(void) { return g_launches.load(std::memory_order_relaxed); }

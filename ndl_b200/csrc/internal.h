@@ -169,6 +169,14 @@ struct FusedParams {
     int zchunk;           // output planes per CTA along Z
     int vec_ld;           // source rows 16-byte aligned with sx == 1
     int vec_st;           // destination rows 4-element aligned with dx == 1
+    // adjoint (input gradient): transposed passes.  zero_pad: out-of-range
+    // samples read as 0 (Clamp/Reflect; Wrap keeps wrapped loads), and the
+    // r = K/2 positions at each end of an axis use the effective weights
+    // z?[e][k] over their K-wide window instead of the flipped taps (rows
+    // e < r: positions 0..r-1; rows r..2r-1: positions n-r..n-1).
+    int adj;
+    int zero_pad;
+    float zx[16][17], zy[16][17], zz[16][17];
     float wxf[64], wyf[64], wzf[64];
     int32_t wxi[64], wyi[64], wzi[64];
 };
@@ -178,7 +186,7 @@ cudaError_t launch_fused(Acc acc, const FusedParams& p, cudaStream_t s);
 bool fused_supported(Acc acc, int src_dtype, int dst_dtype, int kx, int ky, int kz);
 // Float-storage fused kernel with asynchronous loads (fused2.cu).
 cudaError_t launch_fused2(const FusedParams& p, cudaStream_t s);
-bool fused2_supported(int src_dtype, int dst_dtype, int kx, int ky, int kz);
+bool fused2_supported(int src_dtype, int dst_dtype, int kx, int ky, int kz, int adj = 0);
 
 // Sets the per-thread message ndlgpu_last_error() returns; returns s.
 ndlgpu_status set_error(ndlgpu_status s, const std::string& msg);

@@ -366,3 +366,49 @@ def test_adjoint_vs_fp64_oracle(border, dt):
     tref = np.concatenate(taps_ref)
     tscale = np.abs(tref).max()
     assert np.abs(host(tg) - tref).max() <= tol * tscale * 100
+
+
+@pytest.mark.parametrize("border", [0, 1, 2])
+@pytest.mark.parametrize("shape", [(9, 10, 11), (20, 33, 70), (64, 48, 130), (5, 200, 66)])
+def test_fused_adjoint_input_gradient(border, shape):
+    """dL/dX alone runs the fused transposed kernel (zone tables at the
+    borders); checked against the FP64 oracle's literal transpose."""
+    rng = np.random.default_rng(sum(shape) + border)
+    g = rand_array(rng, shape, np.float32)
+    passes = []
+    for ax in range(3):
+        w = rng.standard_normal(9)
+        passes.append((ax, w / np.abs(w).sum()))
+    if border != 0 and min(shape) < 4:
+        pytest.skip("radius exceeds extent")
+    gxi = Image.empty(list(shape[::-1]), torch.float32)
+    n.convolve_axes_adjoint(Image.from_tensor(dev(g)), None, gxi, passes, border, None)
+    gcur = g.astype(np.float64)
+    for ax, w in passes[::-1]:
+        gcur = O.axis_pass_adjoint(gcur, ax, w, border)
+    mag = np.abs(g.astype(np.float64))
+    for ax, w in passes[::-1]:
+        mag = O.axis_pass_adjoint(mag, ax, np.abs(w), border)
+    assert_close(host(gxi.tensor()), gcur, mag, 1e-6, "fused adjoint %s" % (shape,))
+
+
+@pytest.mark.parametrize("tdt", [torch.float32, torch.bfloat16, torch.float16])
+def test_fused_adjoint_video(tdt):
+    rng = np.random.default_rng(9)
+    x = rng.random((7, 3, 40, 70)).astype(np.float32)
+    gx_, gt_ = O.gaussian_weights(2.5), O.gaussian_weights(1.5)
+    passes = [(0, gx_), (1, gx_), (3, gt_)]
+    gi = Image.from_tensor(dev(x).to(tdt))
+    out = Image.empty(gi.extent(), tdt)
+    n.convolve_axes_adjoint(gi, None, out, passes, BorderMode.Reflect, None)
+    code = {torch.float32: O.F32, torch.bfloat16: O.BF16, torch.float16: O.F16}[tdt]
+    gin = O.to_f64(host(gi.tensor()), code)
+    ref = gin
+    for ax, w in passes[::-1]:
+        ref = O.axis_pass_adjoint(ref, ax, w, 2)
+    got = O.to_f64(host(out.tensor()), code)
+    tol = 1e-6 if tdt == torch.float32 else 4e-3
+    mag = np.abs(gin)
+    for ax, w in passes[::-1]:
+        mag = O.axis_pass_adjoint(mag, ax, np.abs(w), 2)
+    assert_close(got, ref, mag, tol, "video adjoint %s" % tdt)
