@@ -140,7 +140,7 @@ struct LPass {
 };
 
 static ndlgpu_status canonicalise(const ndlgpu_view* src, const ndlgpu_view* dst,
-                                  const std::vector<LPass>& lp, int border, Canon* out)
+                                  const std::vector<LPass>& lp, int border, Canon* out, bool keep_zero = false)
 {
     const int R = src->rank;
     if (border < NDLGPU_CLAMP || border > NDLGPU_REFLECT) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "unknown border mode");
@@ -162,7 +162,7 @@ static ndlgpu_status canonicalise(const ndlgpu_view* src, const ndlgpu_view* dst
         CPass cp;
         cp.axis = p.axis;
         for (int k = 0; k < (int)p.taps.size(); k++) {
-            if (p.taps[k] == 0.0) continue;   // image/detail.h:171-172
+            if (p.taps[k] == 0.0 && !keep_zero) continue;   // image/detail.h:171-172
             const int o = k - p.center;
             if (border != NDLGPU_CLAMP && c.total > 0 && (o > src->extent[p.axis] || o < -src->extent[p.axis]))
                 return fail(NDLGPU_ERR_RADIUS_EXCEEDS_EXTENT,
@@ -904,14 +904,132 @@ static bool plan_fused_adjoint(const ndlgpu_view* g, const ndlgpu_view* gx, int 
     return plan_fused(c, Acc::F32, NDLGPU_ROUND_ONCE, border, fp, 1);
 }
 
+// Fused tap gradients: three dense odd-tap passes on distinct axes, X and G
+// of one float type.  Returns false (and leaves no error) when not eligible.
+struct FusedTap {
+    TapFusedParams tp;
+    TapFinalMap map;
+    long long ncta = 0;
+};
+
+static bool plan_fused_tapgrad(const ndlgpu_view* g, const ndlgpu_view* x, int npass,
+                               const ndlgpu_axis_kernel* passes, int border, FusedTap* ft)
+{
+    if (!x || x->dtype != g->dtype) return false;
+    if (x->dtype != NDLGPU_F32 && x->dtype != NDLGPU_BF16 && x->dtype != NDLGPU_F16) return false;
+    if (npass != 3) return false;
+    const std::string keep = t_last_error;
+    std::vector<LPass> lp;
+    if (lpasses_from(npass, passes, &lp) != NDLGPU_OK) { t_last_error = keep; return false; }
+    Canon c;
+    if (canonicalise(x, g, lp, border, &c, true) != NDLGPU_OK || c.total == 0) { t_last_error = keep; return false; }
+    const int R = (int)c.ax.size();
+    std::vector<int> pass_of(R, -1);
+    for (int i = 0; i < 3; i++) {
+        if (pass_of[c.passes[i].axis] >= 0) return false;
+        pass_of[c.passes[i].axis] = i;
+    }
+    if (pass_of[0] < 0) return false;
+    std::vector<int> others;
+    for (int i = 1; i < R; i++)
+        if (pass_of[i] >= 0) others.push_back(i);
+    if (others.size() != 2) return false;
+    const int role[3] = {0, others[0], others[1]};
+    int K[3];
+    for (int r = 0; r < 3; r++) {
+        std::vector<int> o = c.passes[pass_of[role[r]]].off;
+        std::sort(o.begin(), o.end());
+        const int k = (int)o.size();
+        if (k % 2 == 0 || k > 17) return false;
+        for (int i = 0; i < k; i++)
+            if (o[i] != i - k / 2) return false;
+        K[r] = k;
+    }
+    if (!tapgrad_supported(x->dtype, K[0], K[1], K[2])) return false;
+    TapFusedParams& p = ft->tp;
+    std::memset(&p, 0, sizeof(p));
+    p.x = c.src;
+    p.g = c.dst;
+    p.x_dtype = x->dtype;
+    p.border = border;
+    p.zero_pad = border != NDLGPU_WRAP;
+    const CAxis& ax0 = c.ax[role[0]];
+    const CAxis& ay = c.ax[role[1]];
+    const CAxis& az = c.ax[role[2]];
+    p.nx = (int)ax0.n; p.ny = (int)ay.n; p.nz = (int)az.n;
+    p.sx = ax0.ss; p.sy = ay.ss; p.sz = az.ss;
+    p.gxs = ax0.ds; p.gy = ay.ds; p.gz = az.ds;
+    int64_t nb = 1, sb = 0, gb = 0;
+    for (int i = 0; i < R; i++) {
+        if (i == role[0] || i == role[1] || i == role[2]) continue;
+        if (nb == 1) { nb = c.ax[i].n; sb = c.ax[i].ss; gb = c.ax[i].ds; continue; }
+        if (c.ax[i].ss != sb * nb || c.ax[i].ds != gb * nb) return false;
+        nb *= c.ax[i].n;
+    }
+    if (nb > 0x7fffffffLL) return false;
+    p.nbatch = (int)nb;
+    p.sb = sb;
+    p.gb = gb;
+    if ((__int128)(p.ny - 1) * p.sy + (__int128)(p.nx - 1) * p.sx >= ((__int128)1 << 31)) return false;
+    p.kx = K[0]; p.ky = K[1]; p.kz = K[2];
+    const int es = dtype_size(x->dtype);
+    auto al = [](const void* ptr, int64_t bytes) { return ((uintptr_t)ptr % (uintptr_t)bytes) == 0; };
+    p.vec_ld = (p.sx == 1 && al(p.x, 16) && (p.sy * es) % 16 == 0 && (p.sz * es) % 16 == 0 && (p.sb * es) % 16 == 0);
+    p.vec_g = (p.gxs == 1 && al(p.g, 4 * es) && p.gy % 4 == 0 && p.gz % 4 == 0 && p.gb % 4 == 0);
+    // taps ascending by canonical offset; output slot of each: the original
+    // pass and tap index (offsets were negated on axes flipped above)
+    size_t base[3] = {0, 0, 0};
+    {
+        size_t off = 0;
+        for (int i = 0; i < 3; i++) { base[i] = off; off += (size_t)passes[i].ntaps; }
+    }
+    float* wdst[3] = {p.wxf, p.wyf, p.wzf};
+    int t = 0;
+    for (int r = 0; r < 3; r++) {
+        const int pi = pass_of[role[r]];
+        const CPass& cp = c.passes[pi];
+        const int la = passes[pi].axis;
+        const bool flipped = x->stride[la] < 0;
+        std::vector<std::pair<int, double>> tw;
+        for (size_t i = 0; i < cp.off.size(); i++) tw.push_back({cp.off[i], cp.w[i]});
+        std::sort(tw.begin(), tw.end());
+        for (int k = 0; k < K[r]; k++) {
+            wdst[r][k] = (float)tw[k].second;
+            const int o_orig = flipped ? -tw[k].first : tw[k].first;
+            const int k_orig = o_orig + passes[pi].center;
+            if (k_orig < 0 || k_orig >= passes[pi].ntaps) return false;
+            ft->map.dst[t++] = (int)base[pi] + k_orig;
+        }
+    }
+    p.zchunk = tapgrad_zchunk(p.nx, p.ny, p.nz, p.nbatch, p.kz);
+    ft->ncta = tapgrad_ctas(p);
+    return true;
+}
+
 static ndlgpu_status adjoint_execute(const ndlgpu_view* g, const ndlgpu_view* x, const ndlgpu_view* gx,
                                      int border, void* grad_taps, int tdt, const AdjPlan& ap, void* ws,
-                                     size_t ws_bytes, cudaStream_t s, const FusedParams* fused_gx = nullptr)
+                                     size_t ws_bytes, cudaStream_t s, const FusedParams* fused_gx = nullptr,
+                                     FusedTap* fused_tap = nullptr)
 {
     if (ap.total == 0) return NDLGPU_OK;
     if (fused_gx && !grad_taps) {
         cudaError_t e = launch_fused2(*fused_gx, s);
         if (e != cudaSuccess) return cuda_fail(e, "fused adjoint");
+        return NDLGPU_OK;
+    }
+    if (fused_tap && grad_taps && (fused_gx || !gx)) {
+        const size_t need = align_up((size_t)fused_tap->ncta * (fused_tap->tp.kx + fused_tap->tp.ky + fused_tap->tp.kz) *
+                                     sizeof(double));
+        Scratch sc;
+        ndlgpu_status st = get_scratch(need, ws, ws_bytes, s, &sc);
+        if (st != NDLGPU_OK) return st;
+        fused_tap->tp.partial = (double*)sc.base;
+        cudaError_t e = launch_tapgrad(fused_tap->tp, grad_taps, tdt, fused_tap->map, s);
+        if (e != cudaSuccess) return cuda_fail(e, "fused tap gradients");
+        if (fused_gx) {
+            e = launch_fused2(*fused_gx, s);
+            if (e != cudaSuccess) return cuda_fail(e, "fused adjoint");
+        }
         return NDLGPU_OK;
     }
     Scratch sc;
@@ -1240,7 +1358,11 @@ ndlgpu_status ndlgpu_convolve_axes_adjoint_workspace_size(const ndlgpu_view* gra
     ndlgpu_status st = adjoint_prepare(grad_out, src, grad_src, npass, passes, border, src != nullptr,
                                        grad_taps_dtype, &ap);
     if (st != NDLGPU_OK) return st;
-    *bytes = adjoint_workspace(ap);
+    size_t need = adjoint_workspace(ap);
+    FusedTap ft;
+    if (src && ap.total > 0 && plan_fused_tapgrad(grad_out, src, npass, passes, border, &ft))
+        need = std::max(need, align_up((size_t)ft.ncta * (ft.tp.kx + ft.tp.ky + ft.tp.kz) * sizeof(double)));
+    *bytes = need;
     return NDLGPU_OK;
 }
 
@@ -1256,10 +1378,11 @@ ndlgpu_status ndlgpu_convolve_axes_adjoint(const ndlgpu_view* grad_out, const nd
                                        grad_taps_dtype, &ap);
     if (st != NDLGPU_OK) return st;
     FusedParams fp;
-    const bool fused = grad_src && !grad_taps && ap.total > 0 &&
-                       plan_fused_adjoint(grad_out, grad_src, npass, passes, border, &fp);
+    const bool fused = grad_src && ap.total > 0 && plan_fused_adjoint(grad_out, grad_src, npass, passes, border, &fp);
+    FusedTap ft;
+    const bool ftap = grad_taps && ap.total > 0 && plan_fused_tapgrad(grad_out, src, npass, passes, border, &ft);
     return adjoint_execute(grad_out, src, grad_src, border, grad_taps, grad_taps_dtype, ap, workspace,
-                           workspace_bytes, (cudaStream_t)stream, fused ? &fp : nullptr);
+                           workspace_bytes, (cudaStream_t)stream, fused ? &fp : nullptr, ftap ? &ft : nullptr);
 }
 
 uint64_t ndlgpu_kernel_launches(void) { return g_launches.load(std::memory_order_relaxed); }

@@ -194,6 +194,34 @@ ndlgpu_status set_error(ndlgpu_status s, const std::string& msg);
 // Process-wide count of kernel launches (ndlgpu_kernel_launches).
 void count_launch(unsigned n = 1);
 
+// Fused tap gradients of a three-pass chain (tapgrad.cu).  X strides
+// (sx..sb) and G strides (gxs..gb) per canonical role; taps in ascending
+// offset order (forward orientation), every tap present.
+struct TapFusedParams {
+    const char* x;
+    const char* g;
+    double* partial;      // [ncta][kx + ky + kz]
+    int x_dtype;
+    int border;
+    int zero_pad;         // Clamp / Reflect: G read as zero outside the image
+    int nx, ny, nz, nbatch;
+    int64_t sx, sy, sz, sb;
+    int64_t gxs, gy, gz, gb;
+    int kx, ky, kz;
+    int zchunk;
+    int vec_ld;           // X rows 16-byte aligned, sx == 1
+    int vec_g;            // G rows 4-element aligned, gxs == 1
+    float wxf[64], wyf[64], wzf[64];
+};
+// Output slot of each canonical tap (x taps, then y, then z).
+struct TapFinalMap {
+    int dst[64];
+};
+bool tapgrad_supported(int dt, int kx, int ky, int kz);
+long long tapgrad_ctas(const TapFusedParams& p);
+int tapgrad_zchunk(int nx, int ny, int nz, int nbatch, int kz);
+cudaError_t launch_tapgrad(const TapFusedParams& p, void* out, int out_dtype, const TapFinalMap& mp, cudaStream_t s);
+
 // Device guard word.
 cudaError_t read_device_status(cudaStream_t s, int32_t* code);
 

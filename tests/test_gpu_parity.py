@@ -412,3 +412,53 @@ def test_fused_adjoint_video(tdt):
     for ax, w in passes[::-1]:
         mag = O.axis_pass_adjoint(mag, ax, np.abs(w), 2)
     assert_close(got, ref, mag, tol, "video adjoint %s" % tdt)
+
+
+@pytest.mark.parametrize("border", [0, 1, 2])
+def test_fused_tap_gradients_views_and_batch(border):
+    """Tap gradients through the fused kernel: X seen through a mirrored,
+    axis-swapped view, a batch axis left untouched, every tap reported in the
+    caller's tap order."""
+    rng = np.random.default_rng(31 + border)
+    base = rng.standard_normal((3, 30, 41, 70)).astype(np.float32)     # (b, z, y, x)
+    g = rng.standard_normal((3, 30, 41, 70)).astype(np.float32)
+    taps = [rng.standard_normal(9) for _ in range(3)]
+    xt = dev(base)
+    xi = Image.from_tensor(xt).mirror(0).mirror(2)                       # negative strides on x and z
+    npx = base[:, ::-1, :, ::-1]
+    passes = [(0, taps[0]), (1, taps[1]), (2, taps[2])]
+    tg = torch.zeros(27, dtype=torch.float64, device=DEV)
+    gi = Image.from_tensor(dev(g))
+    gx = Image.empty(gi.extent(), torch.float32)
+    n.convolve_axes_adjoint(gi, xi, gx, passes, border, tg)
+    ref_gx, ref_t = [], []
+    for b in range(3):
+        a, t = O.compose_adjoint(g[b].astype(np.float64), np.ascontiguousarray(npx[b]).astype(np.float64), passes,
+                                 border)
+        ref_gx.append(a)
+        ref_t.append(np.concatenate(t))
+    tref = np.sum(ref_t, axis=0)
+    got = host(tg)
+    assert np.abs(got - tref).max() <= 2e-5 * np.abs(tref).max(), np.abs(got - tref).max() / np.abs(tref).max()
+    gref = np.stack(ref_gx)
+    assert np.abs(host(gx.tensor()) - gref).max() <= 2e-6 * np.abs(gref).max()
+
+
+@pytest.mark.parametrize("tdt", [torch.bfloat16, torch.float16])
+def test_fused_tap_gradients_video_16bit(tdt):
+    rng = np.random.default_rng(77)
+    x = rng.random((12, 2, 40, 72)).astype(np.float32)
+    g = rng.standard_normal((12, 2, 40, 72)).astype(np.float32)
+    gx_, gt_ = O.gaussian_weights(2.5), O.gaussian_weights(1.5)
+    passes = [(0, gx_), (1, gx_), (3, gt_)]
+    xi = Image.from_tensor(dev(x).to(tdt))
+    gi = Image.from_tensor(dev(g).to(tdt))
+    tg = torch.zeros(17 + 17 + 11, dtype=torch.float32, device=DEV)
+    n.convolve_axes_adjoint(gi, xi, None, passes, BorderMode.Reflect, tg)
+    code = O.BF16 if tdt == torch.bfloat16 else O.F16
+    xd = O.to_f64(host(xi.tensor()), code)
+    gd = O.to_f64(host(gi.tensor()), code)
+    _, tref = O.compose_adjoint(gd, xd, passes, 2)
+    tref = np.concatenate(tref)
+    got = host(tg).astype(np.float64)
+    assert np.abs(got - tref).max() <= 1e-4 * np.abs(tref).max()
