@@ -190,6 +190,35 @@ NDLGPU_API ndlgpu_status ndlgpu_convolve_axes_adjoint_workspace_size(const ndlgp
                                                           int npass, const ndlgpu_axis_kernel* passes,
                                                           int border, int grad_taps_dtype, size_t* bytes);
 
+/* ---- batched form (no reference counterpart) ------------------------------
+ * Many images and volumes of uneven extents, tap counts and border modes in
+ * ONE persistent launch.  Each instance is a chain of at most three 1-D
+ * passes on distinct axes of one view (its other axes are left untouched),
+ * with odd, centred tap lists of at most 37 taps, composed like
+ * gaussian_blur() with FP32 accumulation; `adjoint` = 1 runs the transposed
+ * chain (the input gradient of that instance).  All instances of a batch share
+ * one storage type, F32, BF16 or F16 (src and dst alike).  Taps are padded
+ * to compiled widths {1,3,5,9,...,37} with zero weights; inputs are assumed
+ * finite (a padded zero tap multiplies its sample).
+ * Workflow: create, add instances, plan (uploads the instance table and the
+ * work list, ordered by cost), then launch or graph_launch as often as
+ * needed; the instance views keep their addresses between launches.  A
+ * graph_launch captures the launch into a CUDA graph on first use and
+ * replays it afterwards.  tile_config selects one of ndlgpu_batch_tile_configs()
+ * compiled tile shapes (-1: the default). */
+typedef struct ndlgpu_batch ndlgpu_batch;
+NDLGPU_API ndlgpu_status ndlgpu_batch_create(ndlgpu_batch** out);
+NDLGPU_API ndlgpu_status ndlgpu_batch_add(ndlgpu_batch* b, const ndlgpu_view* src, const ndlgpu_view* dst,
+                                          int npass, const ndlgpu_axis_kernel* passes, int border, int adjoint);
+NDLGPU_API ndlgpu_status ndlgpu_batch_plan(ndlgpu_batch* b, int tile_config);
+NDLGPU_API ndlgpu_status ndlgpu_batch_launch(ndlgpu_batch* b, void* stream);
+NDLGPU_API ndlgpu_status ndlgpu_batch_graph_launch(ndlgpu_batch* b, void* stream);
+NDLGPU_API ndlgpu_status ndlgpu_batch_destroy(ndlgpu_batch* b);
+NDLGPU_API int ndlgpu_batch_tile_configs(void);
+NDLGPU_API ndlgpu_status ndlgpu_batch_tile_config_info(int index, int* tile_x, int* tile_y, int* threads);
+/* Instances, work items and total output elements of a planned batch. */
+NDLGPU_API ndlgpu_status ndlgpu_batch_info(const ndlgpu_batch* b, int* instances, int* items, int64_t* elements);
+
 /* ---- allocation-free gaussian_blur ---------------------------------------
  * No counterpart in the reference.  Some callers cannot allocate device
  * memory: plugins hosted by an application that owns the GPU's memory pool

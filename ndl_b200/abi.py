@@ -98,6 +98,15 @@ SIGNATURES = {
     "ndlgpu_device_status": (_I, [_VP, ctypes.POINTER(ctypes.c_int32)]),
     "ndlgpu_kernel_launches": (ctypes.c_uint64, []),
     "ndlgpu_gaussian_blur_noalloc": (_I, [_PV, _PV, ctypes.c_double, _I, _VP]),
+    "ndlgpu_batch_create": (_I, [ctypes.POINTER(_VP)]),
+    "ndlgpu_batch_add": (_I, [_VP, _PV, _PV, _I, _PK, _I, _I]),
+    "ndlgpu_batch_plan": (_I, [_VP, _I]),
+    "ndlgpu_batch_launch": (_I, [_VP, _VP]),
+    "ndlgpu_batch_graph_launch": (_I, [_VP, _VP]),
+    "ndlgpu_batch_destroy": (_I, [_VP]),
+    "ndlgpu_batch_tile_configs": (_I, []),
+    "ndlgpu_batch_tile_config_info": (_I, [_I, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)]),
+    "ndlgpu_batch_info": (_I, [_VP, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_int64)]),
 }
 
 _lib = None

@@ -420,6 +420,34 @@ struct Plan {
 // zero-padded input at j - r + m) collects every tap w_k whose forward read
 // of that input lands on j after the border map (map(i + o_k) == j).  The
 // transposed pass elsewhere is the plain flipped correlation.
+// Zone rows for a transposed pass whose window is W wide (centred) and whose
+// real taps reach r: rows e < r hold positions 0..r-1, rows r..2r-1 hold
+// positions M-r..M-1; entry m weighs the zero-padded input at j - W/2 + m.
+static void zone_rows(int64_t M, int border, const std::vector<std::pair<int, double>>& taps, int W, int r,
+                      std::vector<float>* out)
+{
+    out->assign((size_t)2 * r * W, 0.f);
+    for (int e = 0; e < 2 * r; e++) {
+        const int64_t j = (e < r) ? e : (M - r + (e - r));
+        if (j < 0 || j >= M) continue;
+        for (int m = 0; m < W; m++) {
+            const int64_t i = j - W / 2 + m;
+            if (i < 0 || i >= M) continue;
+            double acc = 0;
+            for (const auto& t : taps) {
+                int64_t pos = i + t.first;
+                if (pos < 0 || pos >= M) {
+                    if (border == NDLGPU_WRAP) pos = pos < 0 ? pos + M : pos - M;
+                    else if (border == NDLGPU_REFLECT) pos = pos < 0 ? -pos - 1 : 2 * M - pos - 1;
+                    else pos = pos < 0 ? 0 : M - 1;
+                }
+                if (pos == j) acc += t.second;
+            }
+            (*out)[(size_t)e * W + m] = (float)acc;
+        }
+    }
+}
+
 static void zone_table(int64_t M, int border, const std::vector<std::pair<int, double>>& taps, int K,
                        float (*tab)[17])
 {
@@ -1124,9 +1152,227 @@ static ndlgpu_status adjoint_execute(const ndlgpu_view* g, const ndlgpu_view* x,
     return NDLGPU_OK;
 }
 
+
+// ---------------------------------------------------------------------------
+// Batched form
+// ---------------------------------------------------------------------------
+
+struct BatchHost {
+    int dtype = -1;
+    std::vector<BatchDesc> descs;
+    std::vector<float> zones;
+    std::vector<int64_t> elems;
+    int cfg = -1;
+    BatchLaunch L{};
+    int nitems = 0;
+    bool planned = false;
+    BatchDesc* d_descs = nullptr;
+    int4* d_items = nullptr;
+    float* d_zones = nullptr;
+    int* d_counter = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    cudaGraph_t graph = nullptr;
+    void release()
+    {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        if (graph) cudaGraphDestroy(graph);
+        gexec = nullptr;
+        graph = nullptr;
+        if (d_descs) cudaFree(d_descs);
+        if (d_items) cudaFree(d_items);
+        if (d_zones) cudaFree(d_zones);
+        if (d_counter) cudaFree(d_counter);
+        d_descs = nullptr;
+        d_items = nullptr;
+        d_zones = nullptr;
+        d_counter = nullptr;
+        planned = false;
+    }
+};
+
+static ndlgpu_status batch_add(BatchHost* b, const ndlgpu_view* src, const ndlgpu_view* dst, int npass,
+                               const ndlgpu_axis_kernel* passes, int border, int adjoint)
+{
+    ndlgpu_status st;
+    if ((st = check_view(src, "src", true)) != NDLGPU_OK) return st;
+    if ((st = check_view(dst, "dst", true)) != NDLGPU_OK) return st;
+    if ((st = check_pair(src, dst)) != NDLGPU_OK) return st;
+    if (src->dtype != dst->dtype || (src->dtype != NDLGPU_F32 && src->dtype != NDLGPU_BF16 && src->dtype != NDLGPU_F16))
+        return fail(NDLGPU_ERR_UNSUPPORTED_DTYPE, "batched instances are F32, BF16 or F16, src and dst alike");
+    if (b->dtype >= 0 && b->dtype != src->dtype)
+        return fail(NDLGPU_ERR_UNSUPPORTED_DTYPE, "all instances of a batch share one storage type");
+    if (border < NDLGPU_CLAMP || border > NDLGPU_REFLECT) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "unknown border mode");
+    if (adjoint != 0 && adjoint != 1) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "adjoint must be 0 or 1");
+    if (npass > 3) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "a batched instance has at most three passes");
+    std::vector<LPass> lp;
+    if ((st = lpasses_from(npass, passes, &lp)) != NDLGPU_OK) return st;
+    Canon c;
+    if ((st = canonicalise(src, dst, lp, border, &c, true)) != NDLGPU_OK) return st;
+    if (c.total == 0) return NDLGPU_OK;
+    const int R = (int)c.ax.size();
+    std::vector<const CPass*> by_axis(R, nullptr);
+    for (auto& p : c.passes) {
+        if (by_axis[p.axis]) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "two passes on one axis of a batched instance");
+        by_axis[p.axis] = &p;
+    }
+    std::vector<int> others;
+    for (int i = 1; i < R; i++)
+        if (by_axis[i]) others.push_back(i);
+    for (int i = 1; i < R && others.size() < 2; i++)
+        if (!by_axis[i] && std::find(others.begin(), others.end(), i) == others.end()) others.push_back(i);
+    std::sort(others.begin(), others.end());
+    int role[3] = {0, others.size() > 0 ? others[0] : -1, others.size() > 1 ? others[1] : -1};
+    BatchDesc d;
+    std::memset(&d, 0, sizeof(d));
+    d.src = c.src;
+    d.dst = c.dst;
+    d.border = border;
+    d.zero_pad = (adjoint && border != NDLGPU_WRAP) ? 1 : 0;
+    d.zone_x = d.zone_y = d.zone_z = -1;
+    int* nn[3] = {&d.nx, &d.ny, &d.nz};
+    long long* ss[3] = {&d.sx, &d.sy, &d.sz};
+    long long* ds[3] = {&d.dx, &d.dy, &d.dz};
+    int* bb[3] = {&d.bx, &d.by, &d.bz};
+    int* rr[3] = {&d.rx, &d.ry, &d.rz};
+    float* ww[3] = {d.wx, d.wy, d.wz};
+    int* zz[3] = {&d.zone_x, &d.zone_y, &d.zone_z};
+    for (int r = 0; r < 3; r++) {
+        if (role[r] < 0) { *nn[r] = 1; *ss[r] = 0; *ds[r] = 0; *bb[r] = 1; *rr[r] = 0; ww[r][0] = 1.f; continue; }
+        const CAxis& a = c.ax[role[r]];
+        if (a.n > 0x7fffffffLL) return fail(NDLGPU_ERR_INDEX_OVERFLOW, "extent too large");
+        *nn[r] = (int)a.n;
+        *ss[r] = a.ss;
+        *ds[r] = a.ds;
+        const CPass* cp = by_axis[role[r]];
+        if (!cp) { *bb[r] = 1; *rr[r] = 0; ww[r][0] = 1.f; continue; }
+        std::vector<std::pair<int, double>> t;
+        for (size_t i = 0; i < cp->off.size(); i++) t.push_back({cp->off[i], cp->w[i]});
+        std::sort(t.begin(), t.end());
+        const int K = (int)t.size();
+        for (int i = 0; i < K; i++)
+            if (K % 2 == 0 || t[i].first != i - K / 2)
+                return fail(NDLGPU_ERR_INVALID_ARGUMENT, "batched passes need odd, centred tap lists");
+        const int B = batch_bucket(K);
+        if (B < 0 || K > kBatchMaxTaps) return fail(NDLGPU_ERR_TOO_MANY_TAPS, "batched passes have at most 37 taps");
+        *bb[r] = B;
+        *rr[r] = K / 2;
+        const int pad = (B - K) / 2;
+        for (int m = 0; m < B; m++) ww[r][m] = 0.f;
+        for (int k = 0; k < K; k++) ww[r][pad + k] = (float)t[k].second;
+        if (adjoint) std::reverse(ww[r], ww[r] + B);
+        if (d.zero_pad && K > 1) {
+            std::vector<float> rows;
+            zone_rows(a.n, border, t, B, K / 2, &rows);
+            *zz[r] = (int)b->zones.size();
+            b->zones.insert(b->zones.end(), rows.begin(), rows.end());
+        }
+    }
+    int64_t nb = 1, sb = 0, db = 0;
+    for (int i = 0; i < R; i++) {
+        if (i == role[0] || i == role[1] || i == role[2]) continue;
+        if (nb == 1) { nb = c.ax[i].n; sb = c.ax[i].ss; db = c.ax[i].ds; continue; }
+        if (c.ax[i].ss != sb * nb || c.ax[i].ds != db * nb)
+            return fail(NDLGPU_ERR_INVALID_ARGUMENT, "the untouched axes of a batched instance must merge into one");
+        nb *= c.ax[i].n;
+    }
+    if (nb > 0x7fffffffLL) return fail(NDLGPU_ERR_INDEX_OVERFLOW, "batch axis too large");
+    d.nb = (int)nb;
+    d.sb = sb;
+    d.db = db;
+    const int es = dtype_size(src->dtype);
+    auto al = [](const void* ptr, int64_t bytes) { return ((uintptr_t)ptr % (uintptr_t)bytes) == 0; };
+    d.vec_ld = (d.sx == 1 && al(d.src, 16) && (d.sy * es) % 16 == 0 && (d.sz * es) % 16 == 0 && (d.sb * es) % 16 == 0);
+    d.vec_st = (d.dx == 1 && al(d.dst, 2 * es) && d.dy % 2 == 0 && d.dz % 2 == 0 && d.db % 2 == 0);
+    b->dtype = src->dtype;
+    b->descs.push_back(d);
+    b->elems.push_back(c.total);
+    b->planned = false;
+    return NDLGPU_OK;
+}
+
+static ndlgpu_status batch_plan(BatchHost* b, int cfg)
+{
+    if (cfg < 0) cfg = 0;
+    if (cfg >= batch_tile_configs()) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "unknown tile configuration");
+    b->release();
+    int tx, ty, nt;
+    batch_tile_info(cfg, &tx, &ty, &nt);
+    int bymax = 1, bzmax = 1;
+    for (auto& d : b->descs) { bymax = std::max(bymax, d.by); bzmax = std::max(bzmax, d.bz); }
+    const int rows_max = ty + bymax - 1;
+    if (b->dtype < 0) b->dtype = NDLGPU_F32;
+    if (batch_smem(b->dtype, cfg, rows_max, bzmax) > 227 * 1024)
+        return fail(NDLGPU_ERR_INVALID_ARGUMENT, "tile configuration too large for the widest taps of this batch");
+    struct It { int4 v; double cost; };
+    std::vector<It> items;
+    for (size_t i = 0; i < b->descs.size(); i++) {
+        BatchDesc& d = b->descs[i];
+        d.ntx = (d.nx + tx - 1) / tx;
+        d.nty = (d.ny + ty - 1) / ty;
+        d.zchunk = std::min(d.nz, std::max(2 * d.bz, 32));
+        d.nzc = (d.nz + d.zchunk - 1) / d.zchunk;
+        for (int bi = 0; bi < d.nb; bi++)
+            for (int t = 0; t < d.ntx * d.nty; t++)
+                for (int z = 0; z < d.nzc; z++) {
+                    const int planes = std::min(d.zchunk, d.nz - z * d.zchunk) + d.bz - 1;
+                    const double cost = (double)tx * ty * planes *
+                                        ((double)d.bx * (ty + d.by - 1) / ty + d.by + d.bz + 4.0);
+                    items.push_back({make_int4((int)i, t, z, bi), cost});
+                }
+    }
+    std::stable_sort(items.begin(), items.end(), [](const It& a, const It& c) { return a.cost > c.cost; });
+    std::vector<int4> iv;
+    for (auto& it : items) iv.push_back(it.v);
+    b->nitems = (int)iv.size();
+    b->cfg = cfg;
+    b->L = BatchLaunch{};
+    b->L.rows_max = rows_max;
+    b->L.ring = bzmax;
+    b->L.nitems = b->nitems;
+    cudaError_t e = batch_prepare(b->dtype, cfg, &b->L);
+    if (e != cudaSuccess) return cuda_fail(e, "batch kernel set-up");
+    const size_t nd = std::max<size_t>(1, b->descs.size()), ni = std::max<size_t>(1, iv.size()),
+                 nz = std::max<size_t>(1, b->zones.size());
+    if ((e = cudaMalloc(&b->d_descs, nd * sizeof(BatchDesc))) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_items, ni * sizeof(int4))) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_zones, nz * sizeof(float))) != cudaSuccess ||
+        (e = cudaMalloc(&b->d_counter, sizeof(int))) != cudaSuccess) {
+        b->release();
+        return cuda_fail(e, "batch tables");
+    }
+    if (!b->descs.empty())
+        e = cudaMemcpy(b->d_descs, b->descs.data(), b->descs.size() * sizeof(BatchDesc), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !iv.empty())
+        e = cudaMemcpy(b->d_items, iv.data(), iv.size() * sizeof(int4), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !b->zones.empty())
+        e = cudaMemcpy(b->d_zones, b->zones.data(), b->zones.size() * sizeof(float), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        b->release();
+        return cuda_fail(e, "batch table upload");
+    }
+    b->L.descs = b->d_descs;
+    b->L.items = b->d_items;
+    b->L.zones = b->d_zones;
+    b->L.counter = b->d_counter;
+    b->planned = true;
+    return NDLGPU_OK;
+}
+
+static ndlgpu_status batch_enqueue(BatchHost* b, cudaStream_t s)
+{
+    cudaError_t e = cudaMemsetAsync(b->d_counter, 0, sizeof(int), s);
+    if (e != cudaSuccess) return cuda_fail(e, "batch counter reset");
+    if (b->nitems == 0) return NDLGPU_OK;
+    e = launch_batch(b->dtype, b->cfg, b->L, s);
+    if (e != cudaSuccess) return cuda_fail(e, "batch launch");
+    return NDLGPU_OK;
+}
+
 }  // namespace ndlgpu
 
 using namespace ndlgpu;
+
+struct ndlgpu_batch : ndlgpu::BatchHost {};
 
 extern "C" {
 
@@ -1383,6 +1629,93 @@ ndlgpu_status ndlgpu_convolve_axes_adjoint(const ndlgpu_view* grad_out, const nd
     const bool ftap = grad_taps && ap.total > 0 && plan_fused_tapgrad(grad_out, src, npass, passes, border, &ft);
     return adjoint_execute(grad_out, src, grad_src, border, grad_taps, grad_taps_dtype, ap, workspace,
                            workspace_bytes, (cudaStream_t)stream, fused ? &fp : nullptr, ftap ? &ft : nullptr);
+}
+
+ndlgpu_status ndlgpu_batch_create(ndlgpu_batch** out)
+{
+    t_last_error.clear();
+    if (!out) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = new ndlgpu_batch();
+    return NDLGPU_OK;
+}
+
+ndlgpu_status ndlgpu_batch_add(ndlgpu_batch* b, const ndlgpu_view* src, const ndlgpu_view* dst, int npass,
+                               const ndlgpu_axis_kernel* passes, int border, int adjoint)
+{
+    t_last_error.clear();
+    if (!b) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "batch is NULL");
+    return batch_add(b, src, dst, npass, passes, border, adjoint);
+}
+
+ndlgpu_status ndlgpu_batch_plan(ndlgpu_batch* b, int tile_config)
+{
+    t_last_error.clear();
+    if (!b) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "batch is NULL");
+    return batch_plan(b, tile_config);
+}
+
+ndlgpu_status ndlgpu_batch_launch(ndlgpu_batch* b, void* stream)
+{
+    t_last_error.clear();
+    if (!b || !b->planned) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "batch is NULL or not planned");
+    return batch_enqueue(b, (cudaStream_t)stream);
+}
+
+ndlgpu_status ndlgpu_batch_graph_launch(ndlgpu_batch* b, void* stream)
+{
+    t_last_error.clear();
+    if (!b || !b->planned) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "batch is NULL or not planned");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!b->gexec) {
+        if (!s) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "graph capture needs a non-default stream");
+        cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamBeginCapture");
+        ndlgpu_status st = batch_enqueue(b, s);
+        cudaGraph_t g = nullptr;
+        e = cudaStreamEndCapture(s, &g);
+        if (st != NDLGPU_OK) { if (g) cudaGraphDestroy(g); return st; }
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+        e = cudaGraphInstantiate(&b->gexec, g, 0);
+        if (e != cudaSuccess) { cudaGraphDestroy(g); return cuda_fail(e, "cudaGraphInstantiate"); }
+        b->graph = g;
+    }
+    cudaError_t e = cudaGraphLaunch(b->gexec, s);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGraphLaunch");
+    return NDLGPU_OK;
+}
+
+ndlgpu_status ndlgpu_batch_destroy(ndlgpu_batch* b)
+{
+    t_last_error.clear();
+    if (!b) return NDLGPU_OK;
+    b->release();
+    delete b;
+    return NDLGPU_OK;
+}
+
+int ndlgpu_batch_tile_configs(void) { return batch_tile_configs(); }
+
+ndlgpu_status ndlgpu_batch_tile_config_info(int index, int* tile_x, int* tile_y, int* threads)
+{
+    t_last_error.clear();
+    if (index < 0 || index >= batch_tile_configs() || !tile_x || !tile_y || !threads)
+        return fail(NDLGPU_ERR_INVALID_ARGUMENT, "bad tile configuration index or NULL output");
+    batch_tile_info(index, tile_x, tile_y, threads);
+    return NDLGPU_OK;
+}
+
+ndlgpu_status ndlgpu_batch_info(const ndlgpu_batch* b, int* instances, int* items, int64_t* elements)
+{
+    t_last_error.clear();
+    if (!b) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "batch is NULL");
+    if (instances) *instances = (int)b->descs.size();
+    if (items) *items = b->nitems;
+    if (elements) {
+        int64_t n = 0;
+        for (int64_t v : b->elems) n += v;
+        *elements = n;
+    }
+    return NDLGPU_OK;
 }
 
 uint64_t ndlgpu_kernel_launches(void) { return g_launches.load(std::memory_order_relaxed); }

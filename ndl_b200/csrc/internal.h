@@ -222,6 +222,39 @@ long long tapgrad_ctas(const TapFusedParams& p);
 int tapgrad_zchunk(int nx, int ny, int nz, int nbatch, int kz);
 cudaError_t launch_tapgrad(const TapFusedParams& p, void* out, int out_dtype, const TapFinalMap& mp, cudaStream_t s);
 
+// Batched form (batch.cu): one persistent launch over a table of instances.
+constexpr int kBatchMaxTaps = 37;
+struct BatchDesc {
+    const void* src;
+    void* dst;
+    int nx, ny, nz, nb;
+    long long sx, sy, sz, sb, dx, dy, dz, db;
+    int bx, by, bz;           // compiled tap widths (odd; 1 = no pass)
+    int rx, ry, rz;           // radii of the real taps (adjoint zones)
+    int border, zero_pad, vec_ld, vec_st;
+    int ntx, nty, zchunk, nzc;
+    int zone_x, zone_y, zone_z;   // offsets into the zone-table array (-1: none)
+    float wx[kBatchMaxTaps], wy[kBatchMaxTaps], wz[kBatchMaxTaps];
+};
+struct BatchLaunch {
+    const BatchDesc* descs;
+    const int4* items;
+    int nitems;
+    int* counter;
+    const float* zones;
+    int rows_max;
+    int ring;
+    int grid;
+    size_t smem;
+};
+int batch_tile_configs();
+void batch_tile_info(int i, int* tx, int* ty, int* nt);
+int batch_bucket(int k);
+size_t batch_smem(int dtype, int cfg, int rows_max, int ring);
+// Sets the kernel attributes and the persistent grid (no stream work).
+cudaError_t batch_prepare(int dtype, int cfg, BatchLaunch* L);
+cudaError_t launch_batch(int dtype, int cfg, const BatchLaunch& L, cudaStream_t s);
+
 // Device guard word.
 cudaError_t read_device_status(cudaStream_t s, int32_t* code);
 

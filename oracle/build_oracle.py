@@ -65,9 +65,40 @@ def build_reference(force=False):
     return REF_SO
 
 
+DROPIN_BIN = os.path.join(REF_DIR, "dropin_check")
+
+
+def build_dropin_check(force=False):
+    """tests/cpp/dropin_check.cpp (the C++ drop-in header checked against the
+    reference's own calls) -> oracle/_ref/dropin_check, linked with
+    libndlgpu.so.  Needs the reference tree and a built libndlgpu.so."""
+    repo = os.path.dirname(HERE)
+    src = os.path.join(repo, "tests", "cpp", "dropin_check.cpp")
+    lib_dir = os.path.join(repo, "ndl_b200", "lib")
+    hdrs = [os.path.join(repo, "include", "ndlgpu_dropin.h"), os.path.join(repo, "include", "ndlgpu.h")]
+    if not os.path.isdir(REF_ROOT) or not os.path.exists(os.path.join(lib_dir, "libndlgpu.so")):
+        return DROPIN_BIN if os.path.exists(DROPIN_BIN) else None
+    if not (force or _stale(DROPIN_BIN, [src] + hdrs)):
+        return DROPIN_BIN
+    os.makedirs(REF_DIR, exist_ok=True)
+    inc = tempfile.mkdtemp(prefix="ndlref_inc_")
+    cuda = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+    try:
+        os.symlink(REF_ROOT, os.path.join(inc, "ndl"))
+        _run(["g++", "-std=c++17", "-O2", "-I", inc, "-I", os.path.join(repo, "include"),
+              "-I", os.path.join(cuda, "include"), "-o", DROPIN_BIN, src,
+              "-L", lib_dir, "-lndlgpu", "-Wl,-rpath,$ORIGIN/../../ndl_b200/lib",
+              "-L", os.path.join(cuda, "lib64"), "-lcudart_static", "-ldl", "-lrt", "-lpthread"])
+    finally:
+        shutil.rmtree(inc, ignore_errors=True)
+    return DROPIN_BIN
+
+
 def build(force=False):
     build_restatement(force)
-    return build_reference(force)
+    ref = build_reference(force)
+    build_dropin_check(force)
+    return ref
 
 
 if __name__ == "__main__":
