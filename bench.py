@@ -339,6 +339,10 @@ def other_forms(args, hbm):
         out[name] = {"ms": round(ms, 3), "gvoxel_s": round(vox / ms / 1e6, 2), "gbs": round(2.0 * es * vox / ms / 1e6, 1),
                      "frac_of_measured_hbm": round(2.0 * es * vox / ms / 1e6 / hbm, 4)}
         del v, s, o, salt
+    # config 4: 512 uneven instances, one persistent launch (graph replay),
+    # FP32 and BF16 storage, forward and adjoint; against the plain per-call
+    # FP32 path on the same instances
+    out.update(batched_forms(hbm))
     # config 1: 2-D 512^2 gaussian sigma 2 (L2-resident; launch-bound)
     im = torch.rand((512, 512), generator=g, device="cuda")
     s = Image.from_tensor(im)
@@ -348,6 +352,85 @@ def other_forms(args, hbm):
                               "note": "2 MB, L2-resident and launch-bound"}
     torch.cuda.empty_cache()
     return out
+
+
+def config4_instances(seed=SEED):
+    """512 instances: 256 2-D images with sides log-uniform in [64, 2048] and
+    256 3-D volumes with sides log-uniform in [32, 160]; per axis a Gaussian
+    sigma uniform in [0.5, 6] (radius ceil(3 sigma)); border uniform over
+    Clamp/Wrap/Reflect; values uniform [0, 1)."""
+    from ndl_b200.convolution import gaussian_taps
+    rng = np.random.default_rng(seed)
+    inst = []
+    for i in range(512):
+        if i < 256:
+            shape = tuple(int(round(v)) for v in np.exp(rng.uniform(np.log(64), np.log(2048), 2)))
+        else:
+            shape = tuple(int(round(v)) for v in np.exp(rng.uniform(np.log(32), np.log(160), 3)))
+        border = int(rng.integers(0, 3))
+        passes = [(ax, gaussian_taps(float(rng.uniform(0.5, 6.0)))) for ax in range(len(shape))]
+        inst.append((shape, passes, border))
+    return inst
+
+
+def batched_forms(hbm):
+    import torch
+
+    import ndl_b200 as n
+    from ndl_b200 import Image
+    from ndl_b200.autotune import best_tile_config
+    from ndl_b200.batch import Batch
+
+    res = {}
+    inst = config4_instances()
+    elems = sum(int(np.prod(sh)) for sh, _, _ in inst)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(SEED)
+    stream = torch.cuda.Stream()
+    for name, dt in (("f32", torch.float32), ("bf16", torch.bfloat16)):
+        xs = [torch.rand(sh, generator=g, device="cuda", dtype=torch.float32).to(dt) for sh, _, _ in inst]
+        ys = [torch.empty_like(x) for x in xs]
+        gs = [torch.empty_like(x) for x in xs]
+        xi = [Image.from_tensor(x) for x in xs]
+        yi = [Image.from_tensor(y) for y in ys]
+        gi = [Image.from_tensor(v) for v in gs]
+        fwd, adj = Batch(), Batch()
+        for (sh, passes, border), a, b, c in zip(inst, xi, yi, gi):
+            fwd.add(a, b, passes, border)
+            adj.add(b, c, passes, border, adjoint=True)
+        cfg_f, _ = best_tile_config(fwd)
+        cfg_a, _ = best_tile_config(adj)
+        for tag, b in (("fwd", fwd), ("adj", adj)):
+            with torch.cuda.stream(stream):
+                for _ in range(3):
+                    b.graph_launch(stream)
+                stream.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                for _ in range(5):
+                    b.graph_launch(stream)
+                e1.record(stream)
+                stream.synchronize()
+            ms = e0.elapsed_time(e1) / 5
+            es = xs[0].element_size()
+            res["batched_%s_%s" % (name, tag)] = {
+                "ms": round(ms, 3), "gvoxel_s": round(elems / ms / 1e6, 2),
+                "gbs": round(2.0 * es * elems / ms / 1e6, 1),
+                "frac_of_measured_hbm": round(2.0 * es * elems / ms / 1e6 / hbm, 4),
+                "instances": 512, "elements": elems, "tile_config": cfg_f if tag == "fwd" else cfg_a}
+        if name == "f32":
+            # the plain path: one convolve_axes call per instance (FP32)
+            def plain():
+                for (sh, passes, border), a, b in zip(inst, xi, yi):
+                    n.convolve_axes(a, b, passes, border)
+            ms = time_call(plain, 3, warm=1)
+            res["plain_f32_fwd_per_call"] = {"ms": round(ms, 3), "gvoxel_s": round(elems / ms / 1e6, 2),
+                                             "instances": 512, "elements": elems}
+        fwd.close()
+        adj.close()
+        del xs, ys, gs, xi, yi, gi
+        torch.cuda.empty_cache()
+    return res
 
 
 # ---------------------------------------------------------------------------

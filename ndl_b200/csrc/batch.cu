@@ -69,20 +69,6 @@ __device__ __forceinline__ int zone_row(int j, int n, int r)
     return -1;
 }
 
-// Shared-memory layout of one CTA, from the launch-wide maxima.
-struct Lay {
-    int pitch;        // elements per input row (TX + 48)
-    int rows;         // TY + widest Y bucket - 1
-    int ring;         // widest Z bucket
-    size_t in_off, x_off, ring_off, w_off;
-};
-
-template <class T, int TX, int TY>
-struct Item {
-    static constexpr int NT = TX * TY / 2;
-    static constexpr int EPC = 16 / (int)sizeof(T);
-};
-
 // X pass with a compiled width B (taps at offsets -B/2..B/2).
 template <class T, int TX, int B>
 __device__ __forceinline__ void xpass(const T* sb, float* s_x, const float* s_w, int rows, int pitch, int nt,
@@ -247,7 +233,12 @@ __global__ void __launch_bounds__(TX * TY / 2) k_batch(const BatchDesc* __restri
         auto issue = [&](int zi, int stage) {
             T* sb = s_in + stage * stage_elems;
             const bool zplane = d.zero_pad && (zi < 0 || zi >= d.nz);
-            const int zm = zplane ? 0 : map_border32(d.border, d.nz, zi);
+            // planes beyond the real tap radius feed only zero-padded taps:
+            // any plane inside the image will do (the padded radius can
+            // exceed the extent, where the border map is not defined)
+            const int zm = zplane ? 0
+                         : (zi < -d.rz || zi >= d.nz + d.rz) ? (zi < 0 ? 0 : d.nz - 1)
+                                                             : map_border32(d.border, d.nz, zi);
             const T* pl = src + (int64_t)zm * d.sz;
             for (int t = tid; t < rows * nch; t += NT) {
                 const int r = t / nch, q = t - (t / nch) * nch;
@@ -259,7 +250,7 @@ __global__ void __launch_bounds__(TX * TY / 2) k_batch(const BatchDesc* __restri
                     for (int e = 0; e < EPC; e++) sd[e] = from_f<T>(0.f);
                     continue;
                 }
-                y = (y >= d.ny + d.by - 1 - cby) ? d.ny - 1 : map_border32(d.border, d.ny, y);
+                y = (y < -d.ry || y >= d.ny + d.ry) ? d.ny - 1 : map_border32(d.border, d.ny, y);
                 const T* row = pl + (int64_t)y * d.sy;
                 const int cx0 = gx0 + q * EPC;
                 if (d.vec_ld && cx0 >= 0 && cx0 + EPC <= d.nx) {
@@ -269,7 +260,7 @@ __global__ void __launch_bounds__(TX * TY / 2) k_batch(const BatchDesc* __restri
                     for (int e = 0; e < EPC; e++) {
                         int x = cx0 + e;
                         if (d.zero_pad && (x < 0 || x >= d.nx)) { sd[e] = from_f<T>(0.f); continue; }
-                        x = (x >= d.nx + d.bx - 1 - cbx || x < -cbx) ? d.nx - 1 : map_border32(d.border, d.nx, x);
+                        x = (x < -d.rx || x >= d.nx + d.rx) ? d.nx - 1 : map_border32(d.border, d.nx, x);
                         if constexpr (sizeof(T) == 4) cp_async4(sd + e, row + (int64_t)x * d.sx);
                         else sd[e] = row[(int64_t)x * d.sx];
                     }

@@ -122,24 +122,27 @@ struct Geo {
 // Output plane sum of the Z queue for the newest slot S: tap k reads slot
 // (S + 1 + k) mod KZ (the queue holds the last KZ planes in ring order).
 template <int KZ, int S>
-__device__ __forceinline__ void zstep(float (&q)[KZ][8], const float (&yv)[8], float (&out)[8], const FusedParams& p,
-                                      int ez)
+__device__ __forceinline__ void zstep(float2 (&q)[KZ][4], const float2 (&yv)[4], float2 (&out)[4],
+                                      const FusedParams& p, int ez)
 {
 #pragma unroll
-    for (int e = 0; e < 8; e++) q[S][e] = yv[e];
+    for (int e = 0; e < 4; e++) q[S][e] = yv[e];
 #pragma unroll
-    for (int e = 0; e < 8; e++) {
-        float a = 0.f;
+    for (int e = 0; e < 4; e++) {
+        float2 a = make_float2(0.f, 0.f);
 #pragma unroll
-        for (int k = 0; k < KZ; k++) a = fmaf(q[(S + 1 + k) % KZ][e], p.wzf[k], a);
+        for (int k = 0; k < KZ; k++) a = __ffma2_rn(q[(S + 1 + k) % KZ][e], p.wz2[k], a);
         out[e] = a;
     }
     if (ez >= 0) {   // adjoint border plane: effective weights
 #pragma unroll
-        for (int e = 0; e < 8; e++) {
-            float a = 0.f;
+        for (int e = 0; e < 4; e++) {
+            float2 a = make_float2(0.f, 0.f);
 #pragma unroll
-            for (int k = 0; k < KZ; k++) a = fmaf(q[(S + 1 + k) % KZ][e], p.zz[ez][k], a);
+            for (int k = 0; k < KZ; k++) {
+                const float w = p.zz[ez][k];
+                a = __ffma2_rn(q[(S + 1 + k) % KZ][e], make_float2(w, w), a);
+            }
             out[e] = a;
         }
     }
@@ -155,7 +158,7 @@ __device__ __forceinline__ int zone_row(int j, int n, int r)
 }
 
 template <int KZ>
-__device__ __forceinline__ void zdispatch(int slot, float (&q)[KZ][8], const float (&yv)[8], float (&out)[8],
+__device__ __forceinline__ void zdispatch(int slot, float2 (&q)[KZ][4], const float2 (&yv)[4], float2 (&out)[4],
                                           const FusedParams& p, int ez)
 {
 #define NDLGPU_ZCASE(S) \
@@ -175,8 +178,14 @@ __device__ __forceinline__ void zdispatch(int slot, float (&q)[KZ][8], const flo
 #undef NDLGPU_ZCASE
 }
 
+// CTAs per SM: the adjoint's border-zone paths need more registers.
+template <int TY, bool ADJ>
+struct Occ {
+    static constexpr int value = TY <= 16 ? (ADJ ? 3 : 4) : 2;
+};
+
 template <class Tin, class Tout, int KX, int KY, int KZ, int TY, bool ADJ>
-__global__ void __launch_bounds__(8 * TY, (TY <= 16 ? 4 : 2)) k_fused2(const __grid_constant__ FusedParams p)
+__global__ void __launch_bounds__(8 * TY, (Occ<TY, ADJ>::value)) k_fused2(const __grid_constant__ FusedParams p)
 {
     using G = Geo<Tin, KX, KY, TY>;
     constexpr int NT = G::NT;
@@ -283,11 +292,11 @@ __global__ void __launch_bounds__(8 * TY, (TY <= 16 ? 4 : 2)) k_fused2(const __g
 
     const int gx = tid & 15;
     const int gy = tid >> 4;
-    float q[KZ][8];
+    float2 q[KZ][4];
 #pragma unroll
     for (int k = 0; k < KZ; k++)
 #pragma unroll
-        for (int e = 0; e < 8; e++) q[k][e] = 0.f;
+        for (int e = 0; e < 4; e++) q[k][e] = make_float2(0.f, 0.f);
 
     int slot = 0;
     for (int n = 0; n < nplanes; n++) {
@@ -331,20 +340,19 @@ __global__ void __launch_bounds__(8 * TY, (TY <= 16 ? 4 : 2)) k_fused2(const __g
             *reinterpret_cast<float4*>(s_x + r * TX + 4 * g) = make_float4(acc[0], acc[1], acc[2], acc[3]);
         }
         __syncthreads();
-        // Y pass
-        float yv[8];
-#pragma unroll
-        for (int e = 0; e < 8; e++) yv[e] = 0.f;
+        // Y pass (packed pairs of columns): rows 2gy and 2gy+1
+        float2 yv[4] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
 #pragma unroll
         for (int j = 0; j < KY + 1; j++) {
             const float4 v = *reinterpret_cast<const float4*>(s_x + (2 * gy + j) * TX + 4 * gx);
+            const float2 lo = make_float2(v.x, v.y), hi = make_float2(v.z, v.w);
             if (j < KY) {
-                yv[0] = fmaf(v.x, p.wyf[j], yv[0]); yv[1] = fmaf(v.y, p.wyf[j], yv[1]);
-                yv[2] = fmaf(v.z, p.wyf[j], yv[2]); yv[3] = fmaf(v.w, p.wyf[j], yv[3]);
+                yv[0] = __ffma2_rn(lo, p.wy2[j], yv[0]);
+                yv[1] = __ffma2_rn(hi, p.wy2[j], yv[1]);
             }
             if (j >= 1) {
-                yv[4] = fmaf(v.x, p.wyf[j - 1], yv[4]); yv[5] = fmaf(v.y, p.wyf[j - 1], yv[5]);
-                yv[6] = fmaf(v.z, p.wyf[j - 1], yv[6]); yv[7] = fmaf(v.w, p.wyf[j - 1], yv[7]);
+                yv[2] = __ffma2_rn(lo, p.wy2[j - 1], yv[2]);
+                yv[3] = __ffma2_rn(hi, p.wy2[j - 1], yv[3]);
             }
         }
         if (zp) {
@@ -352,21 +360,24 @@ __global__ void __launch_bounds__(8 * TY, (TY <= 16 ? 4 : 2)) k_fused2(const __g
             for (int h = 0; h < 2; h++) {
                 const int e = zone_row(y0 + 2 * gy + h, p.ny, G::CY);
                 if (e < 0) continue;
-                float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+                float2 a0 = make_float2(0.f, 0.f), a1 = make_float2(0.f, 0.f);
 #pragma unroll
                 for (int j = 0; j < KY; j++) {
                     const float4 v = *reinterpret_cast<const float4*>(s_x + (2 * gy + h + j) * TX + 4 * gx);
                     const float w = p.zy[e][j];
-                    a0 = fmaf(v.x, w, a0); a1 = fmaf(v.y, w, a1); a2 = fmaf(v.z, w, a2); a3 = fmaf(v.w, w, a3);
+                    a0 = __ffma2_rn(make_float2(v.x, v.y), make_float2(w, w), a0);
+                    a1 = __ffma2_rn(make_float2(v.z, v.w), make_float2(w, w), a1);
                 }
-                yv[4 * h] = a0; yv[4 * h + 1] = a1; yv[4 * h + 2] = a2; yv[4 * h + 3] = a3;
+                yv[2 * h] = a0;
+                yv[2 * h + 1] = a1;
             }
         }
         // Z pass
-        float out[8];
+        float2 out2[4];
         const int ez = zp ? zone_row(zin0 + n - HZ, p.nz, CZ) : -1;
-        zdispatch<KZ>(slot, q, yv, out, p, ez);
+        zdispatch<KZ>(slot, q, yv, out2, p, ez);
         slot = (slot + 1 == KZ) ? 0 : slot + 1;
+        const float out[8] = {out2[0].x, out2[0].y, out2[1].x, out2[1].y, out2[2].x, out2[2].y, out2[3].x, out2[3].y};
         if (n >= KZ - 1) {
             const int zo = zin0 + n - HZ;
             const int xb = x0 + 4 * gx;
@@ -408,7 +419,7 @@ cudaError_t launch2(const FusedParams& p, cudaStream_t s)
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const long long slots = (long long)sms * (TY <= 16 ? 4 : 2);
+    const long long slots = (long long)sms * Occ<TY, ADJ>::value;
     long long chunks = (slots + gx - 1) / gx;
     int zc = (int)((p.nz + chunks - 1) / chunks);
     zc = max(zc, min(p.nz, 4 * KZ));

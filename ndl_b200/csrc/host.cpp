@@ -602,6 +602,10 @@ static bool plan_fused(const Canon& c, Acc acc, int compose, int border, FusedPa
             zone_table(p.nz, border, sorted(role[2] >= 0 ? by_axis[role[2]] : nullptr), kz, p.zz);
         }
     }
+    for (int k = 0; k < 40; k++) {
+        p.wy2[k] = make_float2(k < ky ? p.wyf[k] : 0.f, k < ky ? p.wyf[k] : 0.f);
+        p.wz2[k] = make_float2(k < kz ? p.wzf[k] : 0.f, k < kz ? p.wzf[k] : 0.f);
+    }
     // 32-bit in-plane offsets in the kernels
     const int ses = dtype_size(c.sdt), des = dtype_size(c.ddt);
     if ((__int128)(p.ny - 1) * (p.sy < 0 ? -p.sy : p.sy) + (__int128)(p.nx - 1) * (p.sx < 0 ? -p.sx : p.sx) >= ((__int128)1 << 31))

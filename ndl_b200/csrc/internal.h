@@ -179,6 +179,7 @@ struct FusedParams {
     float zx[16][17], zy[16][17], zz[16][17];
     float wxf[64], wyf[64], wzf[64];
     int32_t wxi[64], wyi[64], wzi[64];
+    float2 wy2[40], wz2[40];  // (w, w) pairs of the Y and Z taps (packed FP32 FMA)
 };
 
 // Returns cudaErrorNotSupported when no compiled variant matches.
