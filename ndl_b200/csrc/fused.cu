@@ -70,7 +70,7 @@ __device__ __forceinline__ T out_cast(int32_t v, const FusedParams& p)
     return (T)(long long)int_scaled(v, p.shift, p.store_mode);
 }
 
-template <class Tin, class Tout, class A, int KX, int KY, int KZ>
+template <class Tin, class Tout, class A, int KX, int KY, int KZ, bool TS>
 __global__ void __launch_bounds__(NT, 1) k_fused(const __grid_constant__ FusedParams p)
 {
     constexpr int ROWS = TY + KY - 1;
@@ -82,6 +82,8 @@ __global__ void __launch_bounds__(NT, 1) k_fused(const __grid_constant__ FusedPa
 
     __shared__ __align__(16) A s_in[ROWS][PITCH];
     __shared__ __align__(16) A s_x[ROWS][TX];
+    // output plane staged x-major (destination contiguous along Y)
+    __shared__ __align__(16) Tout s_o[TS ? TX : 1][TS ? TY + 4 : 1];
 
     const int tid = threadIdx.x;
     const int ntx = (p.nx + TX - 1) / TX;
@@ -214,15 +216,30 @@ __global__ void __launch_bounds__(NT, 1) k_fused(const __grid_constant__ FusedPa
                 for (int k = 0; k < KZ; k++) a = mac<A>(a, q[k][e], wz<A>(p, k));
                 out[e] = a;
             }
+            if constexpr (TS) {
 #pragma unroll
-            for (int h = 0; h < 2; h++) {
-                const int y = y0 + 2 * gy + h;
-                if (y >= p.ny) continue;
-                const int xb = x0 + 4 * gx;
-                Tout* row = dst + (int64_t)zo * p.dz + (int64_t)y * p.dy;
+                for (int h = 0; h < 2; h++)
 #pragma unroll
-                for (int m = 0; m < 4; m++)
-                    if (xb + m < p.nx) row[(int64_t)(xb + m) * p.dx] = out_cast<Tout>(out[4 * h + m], p);
+                    for (int m = 0; m < 4; m++) s_o[4 * gx + m][2 * gy + h] = out_cast<Tout>(out[4 * h + m], p);
+                __syncthreads();
+                // consecutive threads walk Y: each warp writes one contiguous run
+                Tout* pl = dst + (int64_t)zo * p.dz;
+                for (int t = tid; t < TX * TY; t += NT) {
+                    const int xl = t / TY, yl = t - (t / TY) * TY;
+                    if (x0 + xl < p.nx && y0 + yl < p.ny)
+                        pl[(int64_t)(x0 + xl) * p.dx + (int64_t)(y0 + yl) * p.dy] = s_o[xl][yl];
+                }
+            } else {
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const int y = y0 + 2 * gy + h;
+                    if (y >= p.ny) continue;
+                    const int xb = x0 + 4 * gx;
+                    Tout* row = dst + (int64_t)zo * p.dz + (int64_t)y * p.dy;
+#pragma unroll
+                    for (int m = 0; m < 4; m++)
+                        if (xb + m < p.nx) row[(int64_t)(xb + m) * p.dx] = out_cast<Tout>(out[4 * h + m], p);
+                }
             }
         }
     }
@@ -238,7 +255,8 @@ cudaError_t launch_one(const FusedParams& p, cudaStream_t s)
     const long long gx = (long long)ntx * nty * p.nbatch;
     const int gz = (p.nz + p.zchunk - 1) / p.zchunk;
     if (gx > 0x7fffffffLL || gz > 65535) return cudaErrorInvalidConfiguration;
-    k_fused<Tin, Tout, A, KX, KY, KZ><<<dim3((unsigned)gx, (unsigned)gz), NT, 0, s>>>(p);
+    if (p.tstore) k_fused<Tin, Tout, A, KX, KY, KZ, true><<<dim3((unsigned)gx, (unsigned)gz), NT, 0, s>>>(p);
+    else k_fused<Tin, Tout, A, KX, KY, KZ, false><<<dim3((unsigned)gx, (unsigned)gz), NT, 0, s>>>(p);
     count_launch();
     return cudaGetLastError();
 }

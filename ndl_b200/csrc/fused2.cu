@@ -134,18 +134,7 @@ __device__ __forceinline__ void zstep(float2 (&q)[KZ][4], const float2 (&yv)[4],
         for (int k = 0; k < KZ; k++) a = __ffma2_rn(q[(S + 1 + k) % KZ][e], p.wz2[k], a);
         out[e] = a;
     }
-    if (ez >= 0) {   // adjoint border plane: effective weights
-#pragma unroll
-        for (int e = 0; e < 4; e++) {
-            float2 a = make_float2(0.f, 0.f);
-#pragma unroll
-            for (int k = 0; k < KZ; k++) {
-                const float w = p.zz[ez][k];
-                a = __ffma2_rn(q[(S + 1 + k) % KZ][e], make_float2(w, w), a);
-            }
-            out[e] = a;
-        }
-    }
+    (void)ez;
 }
 
 // Row of the effective-weight table for position j of an axis of extent n
@@ -179,13 +168,13 @@ __device__ __forceinline__ void zdispatch(int slot, float2 (&q)[KZ][4], const fl
 }
 
 // CTAs per SM: the adjoint's border-zone paths need more registers.
-template <int TY, bool ADJ>
+template <int TY, bool ADJ, int KZ>
 struct Occ {
-    static constexpr int value = TY <= 16 ? (ADJ ? 3 : 4) : 2;
+    static constexpr int value = TY <= 16 ? ((ADJ && KZ > 9) ? 3 : 4) : 2;
 };
 
 template <class Tin, class Tout, int KX, int KY, int KZ, int TY, bool ADJ>
-__global__ void __launch_bounds__(8 * TY, (Occ<TY, ADJ>::value)) k_fused2(const __grid_constant__ FusedParams p)
+__global__ void __launch_bounds__(8 * TY, (Occ<TY, ADJ, KZ>::value)) k_fused2(const __grid_constant__ FusedParams p)
 {
     using G = Geo<Tin, KX, KY, TY>;
     constexpr int NT = G::NT;
@@ -323,21 +312,26 @@ __global__ void __launch_bounds__(8 * TY, (Occ<TY, ADJ>::value)) k_fused2(const 
                 for (int k = 0; k < KX; k++) a = fmaf(win[G::WOFF + m + k], p.wxf[k], a);
                 acc[m] = a;
             }
-            if (zp) {
-                const int xg0 = x0 + 4 * g;
-                if (xg0 < G::CX || xg0 + 3 >= p.nx - G::CX) {
-#pragma unroll
-                    for (int m = 0; m < 4; m++) {
-                        const int e = zone_row(xg0 + m, p.nx, G::CX);
-                        if (e < 0) continue;
-                        float a = 0.f;
-#pragma unroll
-                        for (int k = 0; k < KX; k++) a = fmaf(win[G::WOFF + m + k], p.zx[e][k], a);
-                        acc[m] = a;
-                    }
-                }
-            }
             *reinterpret_cast<float4*>(s_x + r * TX + 4 * g) = make_float4(acc[0], acc[1], acc[2], acc[3]);
+        }
+        if (zp && (x0 < G::CX || x0 + TX > p.nx - G::CX)) {
+            // adjoint border columns: effective weights (a separate pass keeps
+            // the main X pass free of these registers)
+            __syncthreads();
+            const int zlo = max(0, G::CX - x0);                 // columns x0 .. x0+zlo-1 are left-zone
+            const int zr0 = max(0, p.nx - G::CX - x0);          // columns from zr0 on are right-zone
+            const int nl = min(zlo, TX), nr = max(0, TX - zr0);
+            for (int t = tid; t < G::ROWS * (nl + nr); t += NT) {
+                const int r = t / (nl + nr), ci = t - r * (nl + nr);
+                const int col = ci < nl ? ci : zr0 + (ci - nl);
+                const int e = zone_row(x0 + col, p.nx, G::CX);
+                if (e < 0 || col >= TX) continue;
+                float a = 0.f;
+#pragma unroll
+                for (int k = 0; k < KX; k++)
+                    a = fmaf(to_f<Tin>(sb[r * G::PITCH + G::D + col + k]), p.zx[e][k], a);
+                s_x[r * TX + col] = a;
+            }
         }
         __syncthreads();
         // Y pass (packed pairs of columns): rows 2gy and 2gy+1
@@ -374,9 +368,39 @@ __global__ void __launch_bounds__(8 * TY, (Occ<TY, ADJ>::value)) k_fused2(const 
         }
         // Z pass
         float2 out2[4];
-        const int ez = zp ? zone_row(zin0 + n - HZ, p.nz, CZ) : -1;
-        zdispatch<KZ>(slot, q, yv, out2, p, ez);
-        slot = (slot + 1 == KZ) ? 0 : slot + 1;
+        if constexpr (ADJ) {
+            // shift-register queue (one copy of the border-plane path)
+#pragma unroll
+            for (int k = 0; k + 1 < KZ; k++)
+#pragma unroll
+                for (int e = 0; e < 4; e++) q[k][e] = q[k + 1][e];
+#pragma unroll
+            for (int e = 0; e < 4; e++) q[KZ - 1][e] = yv[e];
+            const int ez = zp ? zone_row(zin0 + n - HZ, p.nz, CZ) : -1;
+            if (ez < 0) {
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    float2 a = make_float2(0.f, 0.f);
+#pragma unroll
+                    for (int k = 0; k < KZ; k++) a = __ffma2_rn(q[k][e], p.wz2[k], a);
+                    out2[e] = a;
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < 4; e++) {
+                    float2 a = make_float2(0.f, 0.f);
+#pragma unroll
+                    for (int k = 0; k < KZ; k++) {
+                        const float w = p.zz[ez][k];
+                        a = __ffma2_rn(q[k][e], make_float2(w, w), a);
+                    }
+                    out2[e] = a;
+                }
+            }
+        } else {
+            zdispatch<KZ>(slot, q, yv, out2, p, -1);
+            slot = (slot + 1 == KZ) ? 0 : slot + 1;
+        }
         const float out[8] = {out2[0].x, out2[0].y, out2[1].x, out2[1].y, out2[2].x, out2[2].y, out2[3].x, out2[3].y};
         if (n >= KZ - 1) {
             const int zo = zin0 + n - HZ;
@@ -419,12 +443,10 @@ cudaError_t launch2(const FusedParams& p, cudaStream_t s)
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const long long slots = (long long)sms * Occ<TY, ADJ>::value;
-    long long chunks = (slots + gx - 1) / gx;
-    int zc = (int)((p.nz + chunks - 1) / chunks);
-    zc = max(zc, min(p.nz, 4 * KZ));
+    const long long slots = (long long)sms * Occ<TY, ADJ, KZ>::value;
+    const int chunks = pick_zchunks(gx, slots, p.nz, KZ - 1);
     FusedParams pp = p;
-    pp.zchunk = max(1, zc);
+    pp.zchunk = max(1, (p.nz + chunks - 1) / chunks);
     const int gz = (p.nz + pp.zchunk - 1) / pp.zchunk;
     if (gx > 0x7fffffffLL || gz > 65535) return cudaErrorInvalidConfiguration;
     k_fused2<Tin, Tout, KX, KY, KZ, TY, ADJ><<<dim3((unsigned)gx, (unsigned)gz), G::NT, G::SMEM, s>>>(pp);

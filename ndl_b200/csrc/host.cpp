@@ -515,6 +515,17 @@ static bool plan_fused(const Canon& c, Acc acc, int compose, int border, FusedPa
     for (int i = 1; i < R && others.size() < 2; i++)
         if (!by_axis[i] && std::find(others.begin(), others.end(), i) == others.end()) others.push_back(i);
     std::sort(others.begin(), others.end());
+    // integer path: when the destination is contiguous along a non-X pass
+    // axis (a transposed output), make that axis Y and stage the stores
+    bool tstore = false;
+    if (acc == Acc::I32 && !adj && others.size() == 2) {
+        auto ads = [&](int i) { return c.ax[i].ds < 0 ? -c.ax[i].ds : c.ax[i].ds; };
+        const int64_t dx0 = c.ax[0].ds < 0 ? -c.ax[0].ds : c.ax[0].ds;
+        if (dx0 != 1) {
+            if (ads(others[1]) == 1) std::swap(others[0], others[1]);
+            tstore = ads(others[0]) == 1;
+        }
+    }
     if (others.size() >= 1) role[1] = others[0];
     if (others.size() >= 2) role[2] = others[1];
     for (int r = 0; r < 3; r++)
@@ -616,15 +627,15 @@ static bool plan_fused(const Canon& c, Acc acc, int compose, int border, FusedPa
                 (p.sb * ses) % 16 == 0) ? 1 : 0;
     p.vec_st = (p.dx == 1 && al(p.dst, 4 * des) && (p.dy % 4) == 0 && (p.dz % 4) == 0 && (p.db % 4) == 0) ? 1 : 0;
     p.vec_st = v2 ? p.vec_st : 0;
-    // Z chunk: enough CTAs for two waves over the SMs, chunks >= 4*KZ planes
+    p.tstore = tstore ? 1 : 0;
+    // Z chunk of the integer kernel (64 x 32 tiles, two resident CTAs per SM);
+    // the float kernel picks its own at launch
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const long long tiles = (long long)((p.nx + 63) / 64) * ((p.ny + 31) / 32) * p.nbatch;
-    int chunks = (int)std::min<long long>(std::max<long long>(1, (2LL * sms + tiles - 1) / tiles), 65535);
-    int zc = (p.nz + chunks - 1) / chunks;
-    zc = std::max(zc, std::min(p.nz, 4 * kz));
-    p.zchunk = std::max(1, zc);
+    const int chunks = pick_zchunks(tiles, 2LL * sms, p.nz, kz - 1);
+    p.zchunk = std::max(1, (p.nz + chunks - 1) / chunks);
     return true;
 }
 

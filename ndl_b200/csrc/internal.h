@@ -169,6 +169,7 @@ struct FusedParams {
     int zchunk;           // output planes per CTA along Z
     int vec_ld;           // source rows 16-byte aligned with sx == 1
     int vec_st;           // destination rows 4-element aligned with dx == 1
+    int tstore;           // destination contiguous along Y: stores staged through shared memory
     // adjoint (input gradient): transposed passes.  zero_pad: out-of-range
     // samples read as 0 (Clamp/Reflect; Wrap keeps wrapped loads), and the
     // r = K/2 positions at each end of an axis use the effective weights
@@ -191,6 +192,21 @@ bool fused2_supported(int src_dtype, int dst_dtype, int kx, int ky, int kz, int 
 
 // Sets the per-thread message ndlgpu_last_error() returns; returns s.
 ndlgpu_status set_error(ndlgpu_status s, const std::string& msg);
+
+// Number of Z chunks per tile column for a streaming kernel: minimises
+// waves x (planes per chunk + halo planes), a wave being `slots` resident CTAs.
+inline int pick_zchunks(long long tiles, long long slots, int nz, int halo)
+{
+    int best = 1;
+    double best_t = 1e300;
+    for (int c = 1; c <= 64 && c <= nz; c++) {
+        const long long ctas = tiles * c;
+        const long long waves = (ctas + slots - 1) / slots;
+        const double t = (double)waves * ((double)((nz + c - 1) / c) + halo);
+        if (t < best_t * 0.999) { best_t = t; best = c; }
+    }
+    return best;
+}
 
 // Process-wide count of kernel launches (ndlgpu_kernel_launches).
 void count_launch(unsigned n = 1);

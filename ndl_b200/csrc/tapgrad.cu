@@ -89,99 +89,66 @@ struct TGeo {
 
 __device__ __forceinline__ int bmap(int border, int M, int x) { return map_border32(border, M, x); }
 
-// Z-queue step A (before the Y pass): insert G of plane c + r into slot S and
-// form g2 = (Pz^T G)(plane c).  Window position m holds plane c - r + m.
-template <int KZ, int S>
-__device__ __forceinline__ void za(float (&gq)[KZ][4], const float (&gn)[4], float (&g2)[4],
-                                   const TapFusedParams& p, int c)
+// The G queue is a shift register: gq[m] holds plane c - r + m (window
+// position m), gq[KZ-1] the newest.  One copy of the code serves every plane
+// (a rotating-slot dispatch would replicate the border-plane paths KZ times).
+
+// (Pz^T G)(plane c) from the window; border planes (Clamp / Reflect, G zero
+// outside the image) collect, for window plane z_m, every tap k whose
+// forward read map(z_m + o_k) lands on c.
+template <int KZ>
+__device__ __forceinline__ void zt_apply(const float (&gq)[KZ][4], float (&g2)[4], const TapFusedParams& p, int c,
+                                         bool border_plane)
 {
-#pragma unroll
-    for (int e = 0; e < 4; e++) gq[S][e] = gn[e];
-    if (c < 0) return;   // queue prologue: insert only
     constexpr int R = KZ / 2;
-    // interior: plane c - o_k = c - r + m with m = K-1-k
 #pragma unroll
     for (int e = 0; e < 4; e++) {
         float a = 0.f;
 #pragma unroll
-        for (int m = 0; m < KZ; m++) a = fmaf(gq[(S + 1 + m) % KZ][e], p.wzf[KZ - 1 - m], a);
+        for (int m = 0; m < KZ; m++) a = fmaf(gq[m][e], p.wzf[KZ - 1 - m], a);
         g2[e] = a;
     }
-    if (p.zero_pad && (c < R || c >= p.nz - R)) {
-        // border plane: window plane z_m contributes w_k for every tap k with
-        // map(z_m + o_k) == c (z_m inside the image)
+    if (border_plane) {
 #pragma unroll
         for (int e = 0; e < 4; e++) g2[e] = 0.f;
 #pragma unroll
         for (int m = 0; m < KZ; m++) {
             const int z = c - R + m;
-            if (z < 0 || z >= p.nz) continue;
             float coef = 0.f;
+            if (z >= 0 && z < p.nz) {
+                for (int k = 0; k < KZ; k++)
+                    if (map_border32(p.border, p.nz, z + k - R) == c) coef += p.wzf[k];
+            }
 #pragma unroll
-            for (int k = 0; k < KZ; k++)
-                if (bmap(p.border, p.nz, z + k - R) == c) coef += p.wzf[k];
-#pragma unroll
-            for (int e = 0; e < 4; e++) g2[e] = fmaf(gq[(S + 1 + m) % KZ][e], coef, g2[e]);
+            for (int e = 0; e < 4; e++) g2[e] = fmaf(gq[m][e], coef, g2[e]);
         }
     }
 }
 
-// Z-queue step B (after the Y pass): dwz[k] += sum over positions of
-// X2(plane c) * G(plane z) for the planes z with map(z + o_k) == c.
-template <int KZ, int S>
-__device__ __forceinline__ void zb(const float (&gq)[KZ][4], const float (&x2)[4], float (&dwz)[KZ],
-                                   const TapFusedParams& p, int c)
+// dwz[k] += X2(plane c) . G(planes z with map(z + o_k) == c).
+template <int KZ>
+__device__ __forceinline__ void zt_taps(const float (&gq)[KZ][4], const float (&x2)[4], float (&dwz)[KZ],
+                                        const TapFusedParams& p, int c, bool border_plane)
 {
     constexpr int R = KZ / 2;
     float dd[KZ];
 #pragma unroll
-    for (int m = 0; m < KZ; m++) {
-        float a = 0.f;
+    for (int m = 0; m < KZ; m++)
+        dd[m] = fmaf(x2[0], gq[m][0], fmaf(x2[1], gq[m][1], fmaf(x2[2], gq[m][2], x2[3] * gq[m][3])));
+    if (border_plane) {
 #pragma unroll
-        for (int e = 0; e < 4; e++) a = fmaf(x2[e], gq[(S + 1 + m) % KZ][e], a);
-        dd[m] = a;
-    }
-    if (p.zero_pad && (c < R || c >= p.nz - R)) {
-#pragma unroll
-        for (int m = 0; m < KZ; m++) {
-            const int z = c - R + m;
-            if (z < 0 || z >= p.nz) continue;
-#pragma unroll
-            for (int k = 0; k < KZ; k++)
-                if (bmap(p.border, p.nz, z + k - R) == c) dwz[k] += dd[m];
+        for (int k = 0; k < KZ; k++) {
+            float a = 0.f;
+            for (int m = 0; m < KZ; m++) {
+                const int z = c - R + m;
+                if (z >= 0 && z < p.nz && map_border32(p.border, p.nz, z + k - R) == c) a += dd[m];
+            }
+            dwz[k] += a;
         }
     } else {
 #pragma unroll
         for (int k = 0; k < KZ; k++) dwz[k] += dd[KZ - 1 - k];
     }
-}
-
-#define NDLGPU_TCASES(M)                                                                         \
-    M(0) M(1) M(2) M(3) M(4) M(5) M(6) M(7) M(8) M(9) M(10) M(11) M(12) M(13) M(14) M(15) M(16) \
-    M(17) M(18) M(19) M(20) M(21) M(22) M(23) M(24) M(25) M(26) M(27) M(28) M(29) M(30) M(31) M(32)
-
-template <int KZ>
-__device__ __forceinline__ void zdispatch_a(int slot, float (&gq)[KZ][4], const float (&gn)[4], float (&g2)[4],
-                                           const TapFusedParams& p, int c)
-{
-#define NDLGPU_CA(S) \
-    case S:          \
-        if constexpr (S < KZ) za<KZ, (S < KZ ? S : 0)>(gq, gn, g2, p, c); \
-        break;
-    switch (slot) { NDLGPU_TCASES(NDLGPU_CA) default: break; }
-#undef NDLGPU_CA
-}
-
-template <int KZ>
-__device__ __forceinline__ void zdispatch_b(int slot, const float (&gq)[KZ][4], const float (&x2)[4],
-                                           float (&dwz)[KZ], const TapFusedParams& p, int c)
-{
-#define NDLGPU_CB(S) \
-    case S:          \
-        if constexpr (S < KZ) zb<KZ, (S < KZ ? S : 0)>(gq, x2, dwz, p, c); \
-        break;
-    switch (slot) { NDLGPU_TCASES(NDLGPU_CB) default: break; }
-#undef NDLGPU_CB
 }
 
 template <class T, int KX, int KY, int KZ>
@@ -290,17 +257,16 @@ __global__ void __launch_bounds__(NT, 2) k_tapgrad(const __grid_constant__ TapFu
         for (int m = 0; m < KZ; m++)
 #pragma unroll
             for (int e = 0; e < 4; e++) gq[m][e] = 0.f;
-        // queue prologue: planes zs - r .. zs + r - 1 into slots 0 .. KZ-2
-        int slot = 0;
-        {
+        // queue prologue: planes zs - r .. zs + r - 1 into window positions 1 .. KZ-1
+        // (the shift at the first plane moves them to 0 .. KZ-2)
+#pragma unroll
+        for (int m = 1; m < KZ; m++) {
             float v[4];
-            for (int m = 0; m < KZ - 1; m++) {
-                gload(zs - RZ + m, v);
-                float dummy[4];
-                zdispatch_a<KZ>(slot, gq, v, dummy, p, -1);
-                slot = (slot + 1 == KZ) ? 0 : slot + 1;
-            }
+            gload(zs - RZ + m - 1, v);
+#pragma unroll
+            for (int e = 0; e < 4; e++) gq[m][e] = v[e];
         }
+        const bool valid_all = (yg < p.ny) && (xg + 4 <= p.nx);
         const int nplanes = ze - zs;
 #pragma unroll
         for (int s = 0; s < STAGES - 1; s++) {
@@ -347,11 +313,16 @@ __global__ void __launch_bounds__(NT, 2) k_tapgrad(const __grid_constant__ TapFu
                 }
             }
             __syncthreads();
-            // Pz^T G at plane c (queue gets plane c + r)
+            // shift the G window and append plane c + r; then Pz^T G at plane c
+#pragma unroll
+            for (int m = 0; m + 1 < KZ; m++)
+#pragma unroll
+                for (int e = 0; e < 4; e++) gq[m][e] = gq[m + 1][e];
+#pragma unroll
+            for (int e = 0; e < 4; e++) gq[KZ - 1][e] = gn[e];
+            const bool border_plane = p.zero_pad && (c < RZ || c >= p.nz - RZ);
             float g2[4];
-            zdispatch_a<KZ>(slot, gq, gn, g2, p, c);
-            const int qslot = slot;
-            slot = (slot + 1 == KZ) ? 0 : slot + 1;
+            zt_apply<KZ>(gq, g2, p, c, border_plane);
             if (n + 1 < nplanes) gload(c + 1 + RZ, gn);
             // Y pass of Px X -> X2, and dwy
             float x2[4] = {0.f, 0.f, 0.f, 0.f};
@@ -373,11 +344,12 @@ __global__ void __launch_bounds__(NT, 2) k_tapgrad(const __grid_constant__ TapFu
             }
             // positions outside the image carry g2 = 0 but x2 from mapped
             // loads: zero x2 there so that dwz sees no contribution
-            if (yg >= p.ny) { x2[0] = x2[1] = x2[2] = x2[3] = 0.f; }
+            if (!valid_all) {
 #pragma unroll
-            for (int e = 0; e < 4; e++)
-                if (xg + e >= p.nx) x2[e] = 0.f;
-            zdispatch_b<KZ>(qslot, gq, x2, dwz, p, c);
+                for (int e = 0; e < 4; e++)
+                    if (yg >= p.ny || xg + e >= p.nx) x2[e] = 0.f;
+            }
+            zt_taps<KZ>(gq, x2, dwz, p, c, border_plane);
         }
         cp_async_wait<0>();
     }
@@ -405,16 +377,22 @@ __global__ void __launch_bounds__(NT, 2) k_tapgrad(const __grid_constant__ TapFu
     }
 }
 
-// Sum of the per-CTA partials in CTA order; out[map[t]] = sum_t.
+// Sum of the per-CTA partials; out[map[t]] = sum_t.  One warp per tap: lane
+// l adds CTAs l, l+32, ... in order, then a fixed shuffle tree (the same
+// order on every run).
 __global__ void k_tapgrad_final(const double* partial, int ncta, int ntap, TapFinalMap mp, void* out, int out_dtype)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
     if (t >= ntap) return;
     double a = 0.0;
-    for (int c = 0; c < ncta; c++) a += partial[(long long)c * ntap + t];
-    const int o = mp.dst[t];
-    if (out_dtype == NDLGPU_F64) ((double*)out)[o] = a;
-    else ((float*)out)[o] = (float)a;
+    for (int c = lane; c < ncta; c += 32) a += partial[(long long)c * ntap + t];
+    for (int s = 16; s > 0; s >>= 1) a += __shfl_down_sync(0xffffffffu, a, s);
+    if (lane == 0) {
+        const int o = mp.dst[t];
+        if (out_dtype == NDLGPU_F64) ((double*)out)[o] = a;
+        else ((float*)out)[o] = (float)a;
+    }
 }
 
 template <class T, int KX, int KY, int KZ>
@@ -435,7 +413,7 @@ cudaError_t launch_tg(const TapFusedParams& p, void* out, int out_dtype, const T
     if (gx > 0x7fffffffLL || gz > 65535) return cudaErrorInvalidConfiguration;
     k_tapgrad<T, KX, KY, KZ><<<dim3((unsigned)gx, (unsigned)gz), NT, G::SMEM, s>>>(p);
     const int ntap = KX + KY + KZ;
-    k_tapgrad_final<<<1, 64, 0, s>>>(p.partial, (int)(gx * gz), ntap, mp, out, out_dtype);
+    k_tapgrad_final<<<(ntap + 7) / 8, 256, 0, s>>>(p.partial, (int)(gx * gz), ntap, mp, out, out_dtype);
     count_launch(2);
     return cudaGetLastError();
 }
@@ -477,9 +455,8 @@ int tapgrad_zchunk(int nx, int ny, int nz, int nbatch, int kz)
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const long long tiles = (long long)((nx + TX - 1) / TX) * ((ny + TY - 1) / TY) * nbatch;
     const long long slots = 2LL * sms;
-    const long long chunks = (slots + tiles - 1) / tiles;
-    int zc = (int)((nz + chunks - 1) / chunks);
-    zc = zc < 4 * kz ? (nz < 4 * kz ? nz : 4 * kz) : zc;
+    const int chunks = pick_zchunks(tiles, slots, nz, kz - 1);
+    const int zc = (nz + chunks - 1) / chunks;
     return zc < 1 ? 1 : zc;
 }
 
