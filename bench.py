@@ -204,19 +204,45 @@ def run_gpu(args):
     ms_step = total_ms / K
     value = world * voxels / (ms_step * 1e-3) / 1e9
 
-    # roofline of the dominant call (forward: 8 B/voxel; adjoint with tap
-    # gradients: 12 B/voxel, both algorithmic)
     fwd_gbs = 8.0 * voxels / (fwd_ms * 1e-3) / 1e9
     adj_gbs = 12.0 * voxels / (adj_ms * 1e-3) / 1e9
-    if adj_ms >= fwd_ms:
-        dom = {"kernel": "adjoint (dL/dX + 27 tap gradients)", "bytes_per_voxel": 12, "ms": adj_ms, "gbs": adj_gbs}
-    else:
-        dom = {"kernel": "fused forward k_fused<9,9,9>", "bytes_per_voxel": 8, "ms": fwd_ms, "gbs": fwd_gbs}
-    roofline = {"bound": "hbm", "achieved": round(dom["gbs"], 1), "peak": hbm, "unit": "GB/s",
-                "frac": round(dom["gbs"] / hbm, 4), "traffic": None, "kernel": dom["kernel"],
-                "peak_source": peak_src, "traffic_note": "see profiles/ (ncu dram__bytes per launch)"}
 
-    # end to end through the C ABI with host (pinned) buffers
+    # The three kernels of a step, each timed alone (CUDA events on the
+    # launching stream): the forward, dL/dX alone (grad_taps NULL) and the
+    # tap gradients alone (grad_src NULL).  Each moves 8 algorithmic bytes
+    # per voxel: one f32 volume read and one written (forward, dL/dX), or two
+    # f32 volumes read (tap gradients; the per-CTA partial sums are < 1 MB).
+    kern = {}
+    if not args.only:
+        calls = {
+            "k_fused2 forward": fwd,
+            "k_fused2 adjoint dL/dX": lambda: n.convolve_axes_adjoint(wi, xi, gi, passes, BorderMode.Reflect, None,
+                                                                   workspace=wsa, stream=stream),
+            "k_tapgrad tap gradients": lambda: n.convolve_axes_adjoint(wi, xi, None, passes, BorderMode.Reflect,
+                                                                    taps, workspace=wsa, stream=stream),
+        }
+        for name, fn in calls.items():
+            ms = time_call(fn, max(3, min(K, 20)), stream=stream)
+            gbs = 8.0 * voxels / (ms * 1e-3) / 1e9
+            kern[name] = {"ms": round(ms, 4), "gbs": round(gbs, 1), "frac_of_measured_hbm": round(gbs / hbm, 4)}
+    if kern:
+        name = max(kern, key=lambda k: kern[k]["ms"])
+        traffic, tsrc = profiled_traffic(name)
+        roofline = {"bound": "hbm", "achieved": kern[name]["gbs"], "peak": hbm, "unit": "GB/s",
+                    "frac": round(kern[name]["gbs"] / hbm, 4), "traffic": traffic, "kernel": name,
+                    "algorithmic_bytes_per_launch": 8 * voxels, "peak_source": peak_src, "traffic_source": tsrc}
+    else:
+        dom_ms, dom_gbs = (adj_ms, adj_gbs) if adj_ms >= fwd_ms else (fwd_ms, fwd_gbs)
+        roofline = {"bound": "hbm", "achieved": round(dom_gbs, 1), "peak": hbm, "unit": "GB/s",
+                    "frac": round(dom_gbs / hbm, 4), "traffic": None,
+                    "kernel": "adjoint call" if adj_ms >= fwd_ms else "forward call", "peak_source": peak_src}
+
+    # End to end through the C ABI with host (pinned) buffers.  Every step
+    # copies its inputs X, W host->device and its results Y, dL/dX and the
+    # taps device->host.  Steps are pipelined the way a serving loop runs
+    # them: the upload of step k+1, the kernels of step k and the read-back
+    # of step k-1 overlap on three streams (two device buffer sets), so the
+    # sustained rate is set by the slower PCIe direction, not by their sum.
     e2e = None
     if not args.skip_e2e:
         hX = torch.empty(shape, dtype=torch.float32, pin_memory=True)
@@ -227,24 +253,46 @@ def run_gpu(args):
         hG = torch.empty_like(hX, pin_memory=True)
         htaps = torch.empty(3 * NTAP, dtype=torch.float32, pin_memory=True)
         ke = max(3, min(K, 10))
+        sets = [(X, W, Y, GX, taps, xi, wi, yi, gi)]
+        X2, W2, Y2, G2 = (torch.empty_like(X) for _ in range(4))
+        t2 = torch.zeros_like(taps)
+        sets.append((X2, W2, Y2, G2, t2) + tuple(Image.from_tensor(t) for t in (X2, W2, Y2, G2)))
+        s_up, s_cmp, s_dn = torch.cuda.Stream(dev), torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+        ev_up = [torch.cuda.Event() for _ in range(2)]
+        ev_cmp = [torch.cuda.Event() for _ in range(2)]
+        ev_dn = [torch.cuda.Event() for _ in range(2)]
+        for e in ev_cmp + ev_dn:
+            e.record(stream)
 
-        def e2e_step():
-            X.copy_(hX, non_blocking=True)
-            W.copy_(hW, non_blocking=True)
-            fwd()
-            adj()
-            hY.copy_(Y, non_blocking=True)
-            hG.copy_(GX, non_blocking=True)
-            htaps.copy_(taps, non_blocking=True)
+        def e2e_step(k):
+            b = k & 1
+            dX, dW, dY, dG, dT, ix, iw, iy, ig = sets[b]
+            with torch.cuda.stream(s_up):
+                s_up.wait_event(ev_cmp[b])          # inputs of step k-2 consumed
+                dX.copy_(hX, non_blocking=True)
+                dW.copy_(hW, non_blocking=True)
+                ev_up[b].record(s_up)
+            s_cmp.wait_event(ev_up[b])
+            s_cmp.wait_event(ev_dn[b])              # results of step k-2 read back
+            n.convolve_axes(ix, iy, passes, BorderMode.Reflect, workspace=ws, stream=s_cmp)
+            n.convolve_axes_adjoint(iw, ix, ig, passes, BorderMode.Reflect, dT, workspace=wsa, stream=s_cmp)
+            ev_cmp[b].record(s_cmp)
+            with torch.cuda.stream(s_dn):
+                s_dn.wait_event(ev_cmp[b])
+                hY.copy_(dY, non_blocking=True)
+                hG.copy_(dG, non_blocking=True)
+                htaps.copy_(dT, non_blocking=True)
+                ev_dn[b].record(s_dn)
 
-        for _ in range(2):
-            e2e_step()
+        for k in range(2):
+            e2e_step(k)
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        for _ in range(ke):
-            e2e_step()
-        b.record(stream)
+        a.record(s_up)
+        for k in range(ke):
+            e2e_step(k)
+        s_up.wait_stream(s_dn)
+        b.record(s_up)
         torch.cuda.synchronize()
         ems = a.elapsed_time(b) / ke
         if world > 1:
@@ -253,7 +301,9 @@ def run_gpu(args):
             ems = float(t.item())
         e2e = {"value": round(world * voxels / (ems * 1e-3) / 1e9, 3), "unit": "Gvoxel/s",
                "h2d_bytes_per_step": 2 * X.numel() * 4, "d2h_bytes_per_step": 2 * X.numel() * 4 + 3 * NTAP * 4,
-               "ms_per_step": round(ems, 3)}
+               "ms_per_step": round(ems, 3), "steps": ke,
+               "pipeline": "upload k+1 / kernels k / read-back k-1 on three streams, two device buffer sets"}
+        del sets, X2, W2, Y2, G2, t2
 
     forms = {}
     if rank == 0 and not args.skip_forms:
@@ -281,22 +331,50 @@ def run_gpu(args):
                     "gbs": round(fwd_gbs, 1), "frac_of_measured_hbm": round(fwd_gbs / hbm, 4)},
         "adjoint": {"ms": round(adj_ms, 4), "gvoxel_s": round(voxels / adj_ms / 1e6, 2),
                     "gbs": round(adj_gbs, 1), "frac_of_measured_hbm": round(adj_gbs / hbm, 4)},
-        "roofline": roofline, "e2e": e2e, "gpu_launches": int(launches), "clocks": sampler.result(),
+        "kernels": kern, "roofline": roofline, "e2e": e2e, "gpu_launches": int(launches), "clocks": sampler.result(),
         "cpu_baseline": cpu, "forms": forms,
     }
     print(json.dumps(line))
 
 
-def time_call(fn, iters, warm=3):
+PROFILE_OF = {
+    "k_fused2 forward": "k_fused2_fwd_f32_9x9x9_8x192cube.md",
+    "k_fused2 adjoint dL/dX": "k_fused2_adj_f32_9x9x9_8x192cube.md",
+    "k_tapgrad tap gradients": "k_tapgrad_f32_9x9x9_8x192cube.md",
+}
+
+
+def profiled_traffic(kernel):
+    """DRAM bytes (read + write) of one launch of `kernel`, from the
+    committed ncu summary of the same workload (the line
+    'traffic_bytes_per_launch: N'), or (None, why)."""
+    name = PROFILE_OF.get(kernel)
+    if name is None:
+        return None, "no ncu summary for this kernel"
+    path = os.path.join(ROOT, "profiles", name)
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.strip().startswith("traffic_bytes_per_launch:"):
+                    return int(line.split(":", 1)[1].strip()), "profiles/" + name + " (ncu dram__bytes_read+write)"
+    except OSError:
+        pass
+    return None, "profiles/" + name + " missing"
+
+
+def time_call(fn, iters, warm=3, stream=None):
+    """Average device time of fn() over iters calls (CUDA events on the
+    launching stream, after warm untimed calls, synchronised on both sides)."""
     import torch
+    st = stream if stream is not None else torch.cuda.current_stream()
     for _ in range(warm):
         fn()
     torch.cuda.synchronize()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record()
+    a.record(st)
     for _ in range(iters):
         fn()
-    b.record()
+    b.record(st)
     torch.cuda.synchronize()
     return a.elapsed_time(b) / iters
 
@@ -423,7 +501,7 @@ def batched_forms(hbm):
             def plain():
                 for (sh, passes, border), a, b in zip(inst, xi, yi):
                     n.convolve_axes(a, b, passes, border)
-            ms = time_call(plain, 3, warm=1)
+            ms = time_call(plain, 3, warm=3)
             res["plain_f32_fwd_per_call"] = {"ms": round(ms, 3), "gvoxel_s": round(elems / ms / 1e6, 2),
                                              "instances": 512, "elements": elems}
         fwd.close()
@@ -469,13 +547,18 @@ def cpu_sample(depth, seed=SEED):
     return x.size, time.perf_counter() - t0, kind
 
 
-def cpu_baseline_sample():
-    depth = 64
-    vox, sec, kind = cpu_sample(depth)
+def cpu_baseline_sample(volumes=5):
+    """About 10 s of single-thread CPU work: `volumes` 192^3 f32 volumes of
+    the headline step (5 of the 8 a GPU step processes)."""
+    vox, sec, kind = 0, 0.0, "reference"
+    for i in range(volumes):
+        v, s, kind = cpu_sample(EDGE, SEED + i)
+        vox += v
+        sec += s
     return {"value": round(vox / sec / 1e9, 6), "unit": "Gvoxel/s", "cores": 1, "kind": kind,
-            "sample": "one 192x192x%d f32 volume (1/8 of a 192^3 volume), single thread: forward = ndl convolve() "
-                      "x3 (compiled reference, -O3) + adjoint = FP64 oracle port (ndl has no adjoint); %.2f s; %s"
-                      % (depth, sec, _cpu_model())}
+            "sample": "%d f32 volumes of 192^3 (of the 8 per step), single thread: forward = ndl convolve() x3 "
+                      "(compiled reference, -O3) + adjoint = FP64 oracle port (ndl has no adjoint); %.1f s; %s"
+                      % (volumes, sec, _cpu_model())}
 
 
 def run_reference(args):

@@ -614,6 +614,7 @@ static bool plan_fused(const Canon& c, Acc acc, int compose, int border, FusedPa
         }
     }
     for (int k = 0; k < 40; k++) {
+        p.wx2[k] = make_float2(k < kx ? p.wxf[k] : 0.f, k < kx ? p.wxf[k] : 0.f);
         p.wy2[k] = make_float2(k < ky ? p.wyf[k] : 0.f, k < ky ? p.wyf[k] : 0.f);
         p.wz2[k] = make_float2(k < kz ? p.wzf[k] : 0.f, k < kz ? p.wzf[k] : 0.f);
     }
@@ -1043,6 +1044,13 @@ static bool plan_fused_tapgrad(const ndlgpu_view* g, const ndlgpu_view* x, int n
             if (k_orig < 0 || k_orig >= passes[pi].ntaps) return false;
             ft->map.dst[t++] = (int)base[pi] + k_orig;
         }
+    }
+    for (int k = 0; k < 40; k++) {
+        const float wx = k < p.kx ? p.wxf[k] : 0.f, wy = k < p.ky ? p.wyf[k] : 0.f;
+        const float wz = k < p.kz ? p.wzf[p.kz - 1 - k] : 0.f;
+        p.wx2[k] = make_float2(wx, wx);
+        p.wy2[k] = make_float2(wy, wy);
+        p.wzr2[k] = make_float2(wz, wz);
     }
     p.zchunk = tapgrad_zchunk(p.nx, p.ny, p.nz, p.nbatch, p.kz);
     ft->ncta = tapgrad_ctas(p);

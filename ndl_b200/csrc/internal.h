@@ -180,7 +180,7 @@ struct FusedParams {
     float zx[16][17], zy[16][17], zz[16][17];
     float wxf[64], wyf[64], wzf[64];
     int32_t wxi[64], wyi[64], wzi[64];
-    float2 wy2[40], wz2[40];  // (w, w) pairs of the Y and Z taps (packed FP32 FMA)
+    float2 wx2[40], wy2[40], wz2[40];  // (w, w) pairs of the taps (packed FP32 FMA)
 };
 
 // Returns cudaErrorNotSupported when no compiled variant matches.
@@ -229,6 +229,9 @@ struct TapFusedParams {
     int vec_ld;           // X rows 16-byte aligned, sx == 1
     int vec_g;            // G rows 4-element aligned, gxs == 1
     float wxf[64], wyf[64], wzf[64];
+    // (w, w) pairs for packed FP32 FMA: X and Y taps, and the Z taps in
+    // reverse order (window position m of Pz^T G weighs tap kz-1-m)
+    float2 wx2[40], wy2[40], wzr2[40];
 };
 // Output slot of each canonical tap (x taps, then y, then z).
 struct TapFinalMap {
