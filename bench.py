@@ -451,7 +451,10 @@ def config4_instances(seed=SEED):
     return inst
 
 
-def batched_forms(hbm):
+def batched_forms(hbm, count=512, tile=None, plain=True):
+    """Config 4 in one persistent launch per direction (graph replay):
+    the first `count` instances, tiles from the autotuner unless `tile`
+    names a configuration."""
     import torch
 
     import ndl_b200 as n
@@ -460,7 +463,7 @@ def batched_forms(hbm):
     from ndl_b200.batch import Batch
 
     res = {}
-    inst = config4_instances()
+    inst = config4_instances()[:count]
     elems = sum(int(np.prod(sh)) for sh, _, _ in inst)
     g = torch.Generator(device="cuda")
     g.manual_seed(SEED)
@@ -476,8 +479,13 @@ def batched_forms(hbm):
         for (sh, passes, border), a, b, c in zip(inst, xi, yi, gi):
             fwd.add(a, b, passes, border)
             adj.add(b, c, passes, border, adjoint=True)
-        cfg_f, _ = best_tile_config(fwd)
-        cfg_a, _ = best_tile_config(adj)
+        if tile is None:
+            cfg_f, _ = best_tile_config(fwd)
+            cfg_a, _ = best_tile_config(adj)
+        else:
+            fwd.plan(tile)
+            adj.plan(tile)
+            cfg_f = cfg_a = tile
         for tag, b in (("fwd", fwd), ("adj", adj)):
             with torch.cuda.stream(stream):
                 for _ in range(3):
@@ -495,15 +503,15 @@ def batched_forms(hbm):
                 "ms": round(ms, 3), "gvoxel_s": round(elems / ms / 1e6, 2),
                 "gbs": round(2.0 * es * elems / ms / 1e6, 1),
                 "frac_of_measured_hbm": round(2.0 * es * elems / ms / 1e6 / hbm, 4),
-                "instances": 512, "elements": elems, "tile_config": cfg_f if tag == "fwd" else cfg_a}
-        if name == "f32":
+                "instances": len(inst), "elements": elems, "tile_config": cfg_f if tag == "fwd" else cfg_a}
+        if name == "f32" and plain:
             # the plain path: one convolve_axes call per instance (FP32)
             def plain():
                 for (sh, passes, border), a, b in zip(inst, xi, yi):
                     n.convolve_axes(a, b, passes, border)
             ms = time_call(plain, 3, warm=3)
             res["plain_f32_fwd_per_call"] = {"ms": round(ms, 3), "gvoxel_s": round(elems / ms / 1e6, 2),
-                                             "instances": 512, "elements": elems}
+                                             "instances": len(inst), "elements": elems}
         fwd.close()
         adj.close()
         del xs, ys, gs, xi, yi, gi
@@ -610,11 +618,17 @@ def main():
     ap.add_argument("--skip-forms", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--batched-only", type=int, default=0, metavar="N",
+                    help="run only the batched form on the first N config-4 instances (profiling)")
+    ap.add_argument("--batched-tile", type=int, default=None, help="tile configuration instead of the autotuner")
     ap.add_argument("--only", default="", choices=["", "fwd", "adj"],
                     help="time only one half of the step (for profiling captures)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.batched_only:
+        hbm, _ = peaks()
+        print(json.dumps(batched_forms(hbm, args.batched_only, args.batched_tile, plain=False)))
     else:
         run_gpu(args)
 

@@ -73,12 +73,15 @@ struct TGeo {
     static constexpr int ROWS = TY + KY - 1;
     static constexpr int XC = TX + KX - 1;                 // columns of Py X
     static_assert(XC % 4 == 0, "K-1 must be a multiple of 4");
+    static_assert(TY % 4 == 0, "the Y-pass units cover 4 rows");
     static constexpr int NCH = (XC + EPC - 1) / EPC;
     static constexpr int NV = (KX + 3 + 3) / 4;
     static constexpr int WEND = 60 + 4 * NV;
     static constexpr int PITCH = (NCH * EPC > WEND ? NCH * EPC : (WEND + EPC - 1) / EPC * EPC);
     static constexpr int NTASK = (ROWS * NCH + NT - 1) / NT;
-    static constexpr int NU = ROWS * 16 + TY * (XC / 4);    // X-pass and Y-pass units
+    static constexpr int NXU = ROWS * 16;                  // X-pass units: 1 row x 4 columns
+    static constexpr int NQ = XC / 4;
+    static constexpr int NU = NXU + (TY / 4) * NQ;         // + Y-pass units: 4 rows x 4 columns
     static constexpr size_t IN_BYTES = (size_t)STAGES * ROWS * PITCH * sizeof(T);
     static constexpr size_t X1_BYTES = (size_t)ROWS * TX * 4;
     static constexpr size_t X1Y_BYTES = (size_t)(TY * XC + 16) * 4;   // the last windows read past the end
@@ -284,7 +287,7 @@ __global__ void __launch_bounds__(NT, 2) k_tapgrad(const __grid_constant__ TapFu
             const T* sb = s_in + (n % STAGES) * (G::ROWS * G::PITCH);
             // X pass (Px X on all ROWS) and Y pass of the raw tile (Py X on all XC columns)
             for (int u = tid; u < G::NU; u += NT) {
-                if (u < G::ROWS * 16) {
+                if (u < G::NXU) {
                     const int r = u >> 4, g = u & 15;
                     float win[G::NV * 4];
 #pragma unroll
@@ -299,17 +302,32 @@ __global__ void __launch_bounds__(NT, 2) k_tapgrad(const __grid_constant__ TapFu
                     }
                     *reinterpret_cast<float4*>(s_x1 + r * TX + 4 * g) = make_float4(a[0], a[1], a[2], a[3]);
                 } else {
-                    const int v2 = u - G::ROWS * 16;
-                    const int yy = v2 / (G::XC / 4), qq = v2 - yy * (G::XC / 4);
-                    float a[4] = {0.f, 0.f, 0.f, 0.f};
+                    // Py X: 4 rows x 4 columns, each loaded row feeding up to
+                    // 4 outputs (packed FMA over column pairs)
+                    const int v2 = u - G::NXU;
+                    const int rg = v2 / G::NQ, qq = v2 - rg * G::NQ;
+                    const T* col = sb + (4 * rg) * G::PITCH + 4 * qq;
+                    float2 a[4][2];
 #pragma unroll
-                    for (int k = 0; k < KY; k++) {
-                        float w4[4];
-                        lds4(sb + (yy + k) * G::PITCH + 4 * qq, w4);
+                    for (int h = 0; h < 4; h++) a[h][0] = a[h][1] = make_float2(0.f, 0.f);
 #pragma unroll
-                        for (int m = 0; m < 4; m++) a[m] = fmaf(w4[m], p.wyf[k], a[m]);
+                    for (int j = 0; j < KY + 3; j++) {
+                        float t[4];
+                        lds4(col + j * G::PITCH, t);
+                        const float2 lo = make_float2(t[0], t[1]), hi = make_float2(t[2], t[3]);
+#pragma unroll
+                        for (int h = 0; h < 4; h++) {
+                            const int k = j - h;
+                            if (k >= 0 && k < KY) {
+                                a[h][0] = __ffma2_rn(lo, p.wy2[k], a[h][0]);
+                                a[h][1] = __ffma2_rn(hi, p.wy2[k], a[h][1]);
+                            }
+                        }
                     }
-                    *reinterpret_cast<float4*>(s_x1y + yy * G::XC + 4 * qq) = make_float4(a[0], a[1], a[2], a[3]);
+#pragma unroll
+                    for (int h = 0; h < 4; h++)
+                        *reinterpret_cast<float4*>(s_x1y + (4 * rg + h) * G::XC + 4 * qq) =
+                            make_float4(a[h][0].x, a[h][0].y, a[h][1].x, a[h][1].y);
                 }
             }
             __syncthreads();
