@@ -1193,6 +1193,8 @@ struct BatchHost {
     int4* d_items = nullptr;
     float* d_zones = nullptr;
     int* d_counter = nullptr;
+    float* d_scratch = nullptr;
+    size_t counter_ints = 0;
     cudaGraphExec_t gexec = nullptr;
     cudaGraph_t graph = nullptr;
     void release()
@@ -1205,6 +1207,8 @@ struct BatchHost {
         if (d_items) cudaFree(d_items);
         if (d_zones) cudaFree(d_zones);
         if (d_counter) cudaFree(d_counter);
+        if (d_scratch) cudaFree(d_scratch);
+        d_scratch = nullptr;
         d_descs = nullptr;
         d_items = nullptr;
         d_zones = nullptr;
@@ -1259,6 +1263,7 @@ static ndlgpu_status batch_add(BatchHost* b, const ndlgpu_view* src, const ndlgp
     int* rr[3] = {&d.rx, &d.ry, &d.rz};
     float* ww[3] = {d.wx, d.wy, d.wz};
     int* zz[3] = {&d.zone_x, &d.zone_y, &d.zone_z};
+    bool has_pass[3] = {false, false, false};
     for (int r = 0; r < 3; r++) {
         if (role[r] < 0) { *nn[r] = 1; *ss[r] = 0; *ds[r] = 0; *bb[r] = 1; *rr[r] = 0; ww[r][0] = 1.f; continue; }
         const CAxis& a = c.ax[role[r]];
@@ -1277,6 +1282,9 @@ static ndlgpu_status batch_add(BatchHost* b, const ndlgpu_view* src, const ndlgp
                 return fail(NDLGPU_ERR_INVALID_ARGUMENT, "batched passes need odd, centred tap lists");
         const int B = batch_bucket(K);
         if (B < 0 || K > kBatchMaxTaps) return fail(NDLGPU_ERR_TOO_MANY_TAPS, "batched passes have at most 37 taps");
+        if (K / 2 > a.n && border != NDLGPU_CLAMP)
+            return fail(NDLGPU_ERR_INVALID_ARGUMENT, "a Wrap/Reflect pass's radius exceeds its axis extent");
+        has_pass[r] = true;
         *bb[r] = B;
         *rr[r] = K / 2;
         const int pad = (B - K) / 2;
@@ -1290,6 +1298,11 @@ static ndlgpu_status batch_add(BatchHost* b, const ndlgpu_view* src, const ndlgp
             b->zones.insert(b->zones.end(), rows.begin(), rows.end());
         }
     }
+    d.nphase = 0;
+    for (int r = 0; r < 3; r++)
+        if (has_pass[r]) d.pax[d.nphase++] = r;
+    if (d.nphase == 0) d.pax[d.nphase++] = 0;   // no pass: one identity X pass (a copy)
+    d.scr[0] = d.scr[1] = -1;
     int64_t nb = 1, sb = 0, db = 0;
     for (int i = 0; i < R; i++) {
         if (i == role[0] || i == role[1] || i == role[2]) continue;
@@ -1318,48 +1331,75 @@ static ndlgpu_status batch_plan(BatchHost* b, int cfg)
     if (cfg < 0) cfg = 0;
     if (cfg >= batch_tile_configs()) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "unknown tile configuration");
     b->release();
-    int tx, ty, nt;
-    batch_tile_info(cfg, &tx, &ty, &nt);
-    int bymax = 1, bzmax = 1;
-    for (auto& d : b->descs) { bymax = std::max(bymax, d.by); bzmax = std::max(bzmax, d.bz); }
-    const int rows_max = ty + bymax - 1;
+    int kout, warps, nt;
+    batch_tile_info(cfg, &kout, &warps, &nt);
+    const double target = (double)batch_item_outputs(cfg);
     if (b->dtype < 0) b->dtype = NDLGPU_F32;
-    if (batch_smem(b->dtype, cfg, rows_max, bzmax) > 227 * 1024)
-        return fail(NDLGPU_ERR_INVALID_ARGUMENT, "tile configuration too large for the widest taps of this batch");
-    struct It { int4 v; double cost; };
+    // f32 scratch between phases: per instance, one buffer per intermediate,
+    // each 256-byte aligned (an L1 line never spans two instances' buffers)
+    long long off = 0;
+    int bmax = 1;
+    for (auto& d : b->descs) {
+        const long long el = (long long)((d.nx + 3) / 4 * 4) * d.ny * d.nz * d.nb;   // rows padded to 4 floats
+        bmax = std::max(bmax, std::max(d.by, d.bz));
+        const long long al = (el + 63) / 64 * 64;
+        d.scr[0] = d.scr[1] = -1;
+        for (int p = 0; p + 1 < d.nphase; p++) { d.scr[p] = off; off += al; }
+    }
+    // work items: (instance, phase, first unit, units); rows for the X pass,
+    // (64-column block, line, 64-output segment) units for Y and Z
+    struct It { int4 v; int phase; double cost; };
     std::vector<It> items;
+    const int seg = batch_col_unit();
     for (size_t i = 0; i < b->descs.size(); i++) {
         BatchDesc& d = b->descs[i];
-        d.ntx = (d.nx + tx - 1) / tx;
-        d.nty = (d.ny + ty - 1) / ty;
-        d.zchunk = std::min(d.nz, std::max(2 * d.bz, 32));
-        d.nzc = (d.nz + d.zchunk - 1) / d.zchunk;
-        for (int bi = 0; bi < d.nb; bi++)
-            for (int t = 0; t < d.ntx * d.nty; t++)
-                for (int z = 0; z < d.nzc; z++) {
-                    const int planes = std::min(d.zchunk, d.nz - z * d.zchunk) + d.bz - 1;
-                    const double cost = (double)tx * ty * planes *
-                                        ((double)d.bx * (ty + d.by - 1) / ty + d.by + d.bz + 4.0);
-                    items.push_back({make_int4((int)i, t, z, bi), cost});
-                }
+        for (int p = 0; p < d.nphase; p++) {
+            const int a = d.pax[p];
+            const int B = a == 0 ? d.bx : (a == 1 ? d.by : d.bz);
+            long long units, per;
+            double unit_out;
+            if (a == 0) {
+                units = (long long)d.nb * d.nz * d.ny;
+                unit_out = d.nx;
+            } else {
+                const long long n = a == 1 ? d.ny : d.nz;
+                const long long lines = (long long)d.nb * (a == 1 ? d.nz : d.ny);
+                units = (long long)((d.nx + 63) / 64) * lines * ((n + seg - 1) / seg);
+                unit_out = 64.0 * std::min<long long>(n, seg);
+            }
+            // X: rows shared by the warps of a CTA; Y/Z: whole-CTA units
+            per = a == 0 ? std::max<long long>(warps, (long long)std::llround(target / unit_out / warps) * warps)
+                         : std::max<long long>(1, (long long)std::llround(target / unit_out));
+            int cnt = 0;
+            for (long long u = 0; u < units; u += per) {
+                const long long k = std::min(per, units - u);
+                if (u > 0x7fffffffLL) return fail(NDLGPU_ERR_INDEX_OVERFLOW, "batch instance too large");
+                items.push_back({make_int4((int)i, p, (int)u, (int)k), p, (double)k * unit_out * (B + 4)});
+                cnt++;
+            }
+            d.nitems[p] = cnt;
+        }
     }
-    std::stable_sort(items.begin(), items.end(), [](const It& a, const It& c) { return a.cost > c.cost; });
+    std::stable_sort(items.begin(), items.end(), [](const It& a, const It& c) {
+        return a.phase != c.phase ? a.phase < c.phase : a.cost > c.cost;
+    });
     std::vector<int4> iv;
     for (auto& it : items) iv.push_back(it.v);
     b->nitems = (int)iv.size();
     b->cfg = cfg;
     b->L = BatchLaunch{};
-    b->L.rows_max = rows_max;
-    b->L.ring = bzmax;
     b->L.nitems = b->nitems;
+    b->L.stage_bytes = batch_stage_bytes(bmax);
     cudaError_t e = batch_prepare(b->dtype, cfg, &b->L);
     if (e != cudaSuccess) return cuda_fail(e, "batch kernel set-up");
     const size_t nd = std::max<size_t>(1, b->descs.size()), ni = std::max<size_t>(1, iv.size()),
                  nz = std::max<size_t>(1, b->zones.size());
+    b->counter_ints = 2 + 3 * nd;
     if ((e = cudaMalloc(&b->d_descs, nd * sizeof(BatchDesc))) != cudaSuccess ||
         (e = cudaMalloc(&b->d_items, ni * sizeof(int4))) != cudaSuccess ||
         (e = cudaMalloc(&b->d_zones, nz * sizeof(float))) != cudaSuccess ||
-        (e = cudaMalloc(&b->d_counter, sizeof(int))) != cudaSuccess) {
+        (e = cudaMalloc(&b->d_counter, b->counter_ints * sizeof(int))) != cudaSuccess ||
+        (off > 0 && (e = cudaMalloc(&b->d_scratch, (size_t)off * sizeof(float))) != cudaSuccess)) {
         b->release();
         return cuda_fail(e, "batch tables");
     }
@@ -1377,13 +1417,14 @@ static ndlgpu_status batch_plan(BatchHost* b, int cfg)
     b->L.items = b->d_items;
     b->L.zones = b->d_zones;
     b->L.counter = b->d_counter;
+    b->L.scratch = b->d_scratch;
     b->planned = true;
     return NDLGPU_OK;
 }
 
 static ndlgpu_status batch_enqueue(BatchHost* b, cudaStream_t s)
 {
-    cudaError_t e = cudaMemsetAsync(b->d_counter, 0, sizeof(int), s);
+    cudaError_t e = cudaMemsetAsync(b->d_counter, 0, b->counter_ints * sizeof(int), s);
     if (e != cudaSuccess) return cuda_fail(e, "batch counter reset");
     if (b->nitems == 0) return NDLGPU_OK;
     e = launch_batch(b->dtype, b->cfg, b->L, s);

@@ -249,28 +249,36 @@ struct BatchDesc {
     void* dst;
     int nx, ny, nz, nb;
     long long sx, sy, sz, sb, dx, dy, dz, db;
-    int bx, by, bz;           // compiled tap widths (odd; 1 = no pass)
-    int rx, ry, rz;           // radii of the real taps (adjoint zones)
+    int bx, by, bz;           // compiled tap widths (odd; 1 = a single tap)
+    int rx, ry, rz;           // radii of the real taps
     int border, zero_pad, vec_ld, vec_st;
-    int ntx, nty, zchunk, nzc;
+    int nphase;               // passes of this instance, one axis each
+    int pax[3];               // axis of each phase (0 = X, 1 = Y, 2 = Z), ascending
+    int nitems[3];            // work items of each phase (dependency counts)
+    int pad0;
+    long long scr[2];         // element offsets of the f32 scratch after phases 0 and 1 (-1: none)
     int zone_x, zone_y, zone_z;   // offsets into the zone-table array (-1: none)
     float wx[kBatchMaxTaps], wy[kBatchMaxTaps], wz[kBatchMaxTaps];
 };
 struct BatchLaunch {
     const BatchDesc* descs;
-    const int4* items;
+    const int4* items;        // (instance, phase, first unit, units)
     int nitems;
-    int* counter;
+    int* counter;             // [0] next item, [1] error flag, [2 + 3 i + p] finished items
     const float* zones;
-    int rows_max;
-    int ring;
+    float* scratch;
     int grid;
+    int threads;
+    int stage_bytes;          // one column-pass stage (two are resident)
     size_t smem;
 };
 int batch_tile_configs();
 void batch_tile_info(int i, int* tx, int* ty, int* nt);
 int batch_bucket(int k);
-size_t batch_smem(int dtype, int cfg, int rows_max, int ring);
+int batch_item_outputs(int cfg);   // target outputs per work item
+int batch_row_segment();           // row-pass outputs per warp segment
+int batch_col_unit();              // column-pass outputs per unit along the axis
+int batch_stage_bytes(int bmax);   // one column-pass stage for the widest taps
 // Sets the kernel attributes and the persistent grid (no stream work).
 cudaError_t batch_prepare(int dtype, int cfg, BatchLaunch* L);
 cudaError_t launch_batch(int dtype, int cfg, const BatchLaunch& L, cudaStream_t s);
