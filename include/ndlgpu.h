@@ -200,12 +200,19 @@ NDLGPU_API ndlgpu_status ndlgpu_convolve_axes_adjoint_workspace_size(const ndlgp
  * one storage type, F32, BF16 or F16 (src and dst alike).  Taps are padded
  * to compiled widths {1,3,5,9,...,37} with zero weights; inputs are assumed
  * finite (a padded zero tap multiplies its sample).
+ * The launch runs every instance's passes one axis at a time, with FP32
+ * intermediates in device scratch the plan allocates; Wrap/Reflect passes
+ * need their radius within the axis extent (as the reference's one-period
+ * border maps do).
  * Workflow: create, add instances, plan (uploads the instance table and the
- * work list, ordered by cost), then launch or graph_launch as often as
- * needed; the instance views keep their addresses between launches.  A
- * graph_launch captures the launch into a CUDA graph on first use and
- * replays it afterwards.  tile_config selects one of ndlgpu_batch_tile_configs()
- * compiled tile shapes (-1: the default). */
+ * work list, ordered by pass and cost, and allocates the scratch), then
+ * launch or graph_launch as often as needed; the instance views keep their
+ * addresses between launches.  A graph_launch captures the launch into a CUDA
+ * graph on first use and replays it afterwards.  tile_config selects one of
+ * ndlgpu_batch_tile_configs() work-item configurations (-1: the default);
+ * ndlgpu_batch_tile_config_info reports for each the target outputs per work
+ * item in units of 1024 (tile_x), the warps per CTA (tile_y) and the threads
+ * per CTA. */
 typedef struct ndlgpu_batch ndlgpu_batch;
 NDLGPU_API ndlgpu_status ndlgpu_batch_create(ndlgpu_batch** out);
 NDLGPU_API ndlgpu_status ndlgpu_batch_add(ndlgpu_batch* b, const ndlgpu_view* src, const ndlgpu_view* dst,

@@ -19,7 +19,8 @@ from .image import Image
 
 
 def tile_configs():
-    """[(tile_x, tile_y, threads)] of the compiled tile shapes."""
+    """[(k_outputs, warps, threads)] of the work-item configurations: target
+    outputs per work item in units of 1024, warps and threads per CTA."""
     lib = abi.load()
     out = []
     for i in range(lib.ndlgpu_batch_tile_configs()):
