@@ -288,19 +288,29 @@ __global__ void __launch_bounds__(8 * TY, (Occ<TY, ADJ, KZ>::value)) k_fused2(co
         for (int e = 0; e < 4; e++) q[k][e] = make_float2(0.f, 0.f);
 
     int slot = 0;
+    int stage = 0;                       // ring stage of plane n
+    int stage_next = STAGES - 1;         // ring stage of plane n + STAGES - 1
+    // output rows of this thread: row offsets and, per plane, a running
+    // plane pointer (the first output plane is input plane KZ - 1)
+    const int xb = x0 + 4 * gx;
+    int64_t rowoff[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) rowoff[h] = (int64_t)(y0 + 2 * gy + h) * p.dy;
+    Tout* oplane = dst + (int64_t)(zin0 + KZ - 1 - HZ) * p.dz;
     for (int n = 0; n < nplanes; n++) {
         cp_async_wait<STAGES - 2>();
         __syncthreads();    // plane n visible; every thread is past the X pass of plane n-1
-        if (n + STAGES - 1 < nplanes) issue(zin0 + n + STAGES - 1, (n + STAGES - 1) % STAGES);
+        if (n + STAGES - 1 < nplanes) issue(zin0 + n + STAGES - 1, stage_next);
         cp_async_commit();
+        stage_next = (stage_next + 1 == STAGES) ? 0 : stage_next + 1;
 
-        const Tin* sb = s_in + (n % STAGES) * (G::ROWS * G::PITCH);
-        // X pass: ROWS x 16 units of 4 outputs
+        const Tin* sb = s_in + stage * (G::ROWS * G::PITCH);
+        // X pass: ROWS x 16 units of 4 outputs; unit i of this thread is row
+        // gy + i * NT/16, column group gx
 #pragma unroll
         for (int i = 0; i < G::NXU; i++) {
-            const int u = tid + i * NT;
-            if (G::NXU * NT != G::ROWS * 16 && u >= G::ROWS * 16) break;
-            const int r = u >> 4, g = u & 15;
+            if (G::NXU * NT != G::ROWS * 16 && gy + i * (NT / 16) >= G::ROWS) break;
+            const int r = gy + i * (NT / 16), g = gx;
             float win[G::NV * 4];
 #pragma unroll
             for (int v = 0; v < G::NV; v++) lds4(sb + r * G::PITCH + 4 * g + G::WBASE + 4 * v, win + 4 * v);
@@ -402,14 +412,13 @@ __global__ void __launch_bounds__(8 * TY, (Occ<TY, ADJ, KZ>::value)) k_fused2(co
             slot = (slot + 1 == KZ) ? 0 : slot + 1;
         }
         const float out[8] = {out2[0].x, out2[0].y, out2[1].x, out2[1].y, out2[2].x, out2[2].y, out2[3].x, out2[3].y};
+        stage = (stage + 1 == STAGES) ? 0 : stage + 1;
         if (n >= KZ - 1) {
-            const int zo = zin0 + n - HZ;
-            const int xb = x0 + 4 * gx;
 #pragma unroll
             for (int h = 0; h < 2; h++) {
                 const int y = y0 + 2 * gy + h;
                 if (y >= p.ny) continue;
-                Tout* row = dst + (int64_t)zo * p.dz + (int64_t)y * p.dy;
+                Tout* row = oplane + rowoff[h];
                 if (p.vec_st && xb + 4 <= p.nx) {
                     stg4(row + xb, out + 4 * h);
                 } else {
@@ -418,6 +427,7 @@ __global__ void __launch_bounds__(8 * TY, (Occ<TY, ADJ, KZ>::value)) k_fused2(co
                         if (xb + m < p.nx) row[(int64_t)(xb + m) * p.dx] = from_f<Tout>(out[4 * h + m]);
                 }
             }
+            oplane += p.dz;
         }
     }
     cp_async_wait<0>();

@@ -82,6 +82,8 @@ struct TGeo {
     static constexpr int NXU = ROWS * 16;                  // X-pass units: 1 row x 4 columns
     static constexpr int NQ = XC / 4;
     static constexpr int NU = NXU + (TY / 4) * NQ;         // + Y-pass units: 4 rows x 4 columns
+    static constexpr int NUR = (NU + NT - 1) / NT;          // unit rounds per thread
+    static_assert((TY / 4) * NQ <= NT, "one Y unit per thread at most");
     static constexpr size_t IN_BYTES = (size_t)STAGES * ROWS * PITCH * sizeof(T);
     static constexpr size_t X1_BYTES = (size_t)ROWS * TX * 4;
     static constexpr size_t X1Y_BYTES = (size_t)(TY * XC + 16) * 4;   // the last windows read past the end
@@ -168,6 +170,7 @@ __global__ void __launch_bounds__(NT, 2) k_tapgrad(const __grid_constant__ TapFu
                                          G::RED_BYTES);
 
     const int tid = threadIdx.x;
+    __builtin_assume(tid < NT);
     const int ntx = (p.nx + TX - 1) / TX;
     const int nty = (p.ny + TY - 1) / TY;
     const int tile = blockIdx.x % (ntx * nty);
@@ -237,6 +240,7 @@ __global__ void __launch_bounds__(NT, 2) k_tapgrad(const __grid_constant__ TapFu
         // G of this thread's 4 positions: (x0+4gx .. +3, y0+gy)
         const int gxq = tid & 15, gyq = tid >> 4;
         const int xg = x0 + 4 * gxq, yg = y0 + gyq;
+        const T* grow = gs + (int64_t)yg * p.gy;
         auto gload = [&](int zi, float (&v)[4]) {
 #pragma unroll
             for (int e = 0; e < 4; e++) v[e] = 0.f;
@@ -245,7 +249,7 @@ __global__ void __launch_bounds__(NT, 2) k_tapgrad(const __grid_constant__ TapFu
                 if (p.zero_pad) return;
                 zi = bmap(p.border, p.nz, zi);
             }
-            const T* row = gs + (int64_t)zi * p.gz + (int64_t)yg * p.gy;
+            const T* row = grow + (int64_t)zi * p.gz;
             if (p.vec_g && xg + 4 <= p.nx) {
                 lds4(row + xg, v);   // 16- or 8-byte aligned global load
             } else {
@@ -278,17 +282,32 @@ __global__ void __launch_bounds__(NT, 2) k_tapgrad(const __grid_constant__ TapFu
         }
         float gn[4];
         gload(zs + RZ, gn);
+        // this thread's Y unit (if any): v2 = u - NXU for its first u >= NXU
+        int y_rg = 0, y_qq = 0;
+        {
+            const int v2 = tid + ((G::NXU - tid + NT - 1) / NT) * NT - G::NXU;
+            y_rg = v2 / G::NQ;
+            y_qq = v2 - y_rg * G::NQ;
+        }
+        int stage = 0, stage_next = STAGES - 1;
         for (int n = 0; n < nplanes; n++) {
             const int c = zs + n;
             cp_async_wait<STAGES - 2>();
             __syncthreads();
-            if (n + STAGES - 1 < nplanes) issue(zs + n + STAGES - 1, (n + STAGES - 1) % STAGES);
+            if (n + STAGES - 1 < nplanes) issue(zs + n + STAGES - 1, stage_next);
             cp_async_commit();
-            const T* sb = s_in + (n % STAGES) * (G::ROWS * G::PITCH);
-            // X pass (Px X on all ROWS) and Y pass of the raw tile (Py X on all XC columns)
-            for (int u = tid; u < G::NU; u += NT) {
+            stage_next = (stage_next + 1 == STAGES) ? 0 : stage_next + 1;
+            const T* sb = s_in + stage * (G::ROWS * G::PITCH);
+            // X pass (Px X on all ROWS) and Y pass of the raw tile (Py X on
+            // all XC columns).  Unit u = tid + i * NT of this thread: an X
+            // unit (row (tid >> 4) + i * NT/16, column group tid & 15) while
+            // u < NXU, then at most one Y unit (indices set up before the loop)
+#pragma unroll
+            for (int i = 0; i < G::NUR; i++) {
+                const int u = tid + i * NT;
+                if (u >= G::NU) break;
                 if (u < G::NXU) {
-                    const int r = u >> 4, g = u & 15;
+                    const int r = (tid >> 4) + i * (NT / 16), g = tid & 15;
                     float win[G::NV * 4];
 #pragma unroll
                     for (int v = 0; v < G::NV; v++) lds4(sb + r * G::PITCH + 4 * g + 4 * v, win + 4 * v);
@@ -304,8 +323,7 @@ __global__ void __launch_bounds__(NT, 2) k_tapgrad(const __grid_constant__ TapFu
                 } else {
                     // Py X: 4 rows x 4 columns, each loaded row feeding up to
                     // 4 outputs (packed FMA over column pairs)
-                    const int v2 = u - G::NXU;
-                    const int rg = v2 / G::NQ, qq = v2 - rg * G::NQ;
+                    const int rg = y_rg, qq = y_qq;
                     const T* col = sb + (4 * rg) * G::PITCH + 4 * qq;
                     float2 a[4][2];
 #pragma unroll
@@ -368,6 +386,7 @@ __global__ void __launch_bounds__(NT, 2) k_tapgrad(const __grid_constant__ TapFu
                     if (yg >= p.ny || xg + e >= p.nx) x2[e] = 0.f;
             }
             zt_taps<KZ>(gq, x2, dwz, p, c, border_plane);
+            stage = (stage + 1 == STAGES) ? 0 : stage + 1;
         }
         cp_async_wait<0>();
     }
