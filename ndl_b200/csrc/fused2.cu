@@ -287,6 +287,15 @@ __global__ void __launch_bounds__(8 * TY, (Occ<TY, ADJ, KZ>::value)) k_fused2(co
 #pragma unroll
         for (int e = 0; e < 4; e++) q[k][e] = make_float2(0.f, 0.f);
 
+    // adjoint zone rows of this thread's two rows, and whether the tile has
+    // zone columns (both plane-invariant)
+    int ey[2] = {-1, -1};
+    if (zp) {
+#pragma unroll
+        for (int h = 0; h < 2; h++) ey[h] = zone_row(y0 + 2 * gy + h, p.ny, G::CY);
+    }
+    const bool yzone = ey[0] >= 0 || ey[1] >= 0;
+    const bool xzone_tile = zp && (x0 < G::CX || x0 + TX > p.nx - G::CX);
     int slot = 0;
     int stage = 0;                       // ring stage of plane n
     int stage_next = STAGES - 1;         // ring stage of plane n + STAGES - 1
@@ -324,7 +333,7 @@ __global__ void __launch_bounds__(8 * TY, (Occ<TY, ADJ, KZ>::value)) k_fused2(co
             }
             *reinterpret_cast<float4*>(s_x + r * TX + 4 * g) = make_float4(acc[0], acc[1], acc[2], acc[3]);
         }
-        if (zp && (x0 < G::CX || x0 + TX > p.nx - G::CX)) {
+        if (xzone_tile) {
             // adjoint border columns: effective weights (a separate pass keeps
             // the main X pass free of these registers)
             __syncthreads();
@@ -359,10 +368,10 @@ __global__ void __launch_bounds__(8 * TY, (Occ<TY, ADJ, KZ>::value)) k_fused2(co
                 yv[3] = __ffma2_rn(hi, p.wy2[j - 1], yv[3]);
             }
         }
-        if (zp) {
+        if (yzone) {
 #pragma unroll
             for (int h = 0; h < 2; h++) {
-                const int e = zone_row(y0 + 2 * gy + h, p.ny, G::CY);
+                const int e = ey[h];
                 if (e < 0) continue;
                 float2 a0 = make_float2(0.f, 0.f), a1 = make_float2(0.f, 0.f);
 #pragma unroll
