@@ -379,6 +379,33 @@ def time_call(fn, iters, warm=3, stream=None):
     return a.elapsed_time(b) / iters
 
 
+def video_error(dt, seed=SEED):
+    """Error of the configuration-5 blur in storage type dt against the FP64
+    oracle, on a 96 x 3 x 128 x 128 (t, c, y, x) crop with the same value
+    distribution (the GPU and the oracle see the same decoded inputs; data and
+    taps are positive, so the stencil magnitude is the exact result)."""
+    import torch
+
+    import ndl_b200 as n
+    from ndl_b200 import BorderMode, Image
+    from oracle import oracle as O
+
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed + 5)
+    v = torch.rand((96, 3, 128, 128), generator=g, device="cuda")
+    v[torch.rand(v.shape, generator=g, device="cuda") < 0.01] = 1.0
+    v = v.to(dt)
+    o = Image.empty(Image.from_tensor(v).extent(), dt)
+    sig = (2.5, 2.5, 0.0, 1.5)
+    n.gaussian_blur_axes(Image.from_tensor(v), o, list(sig), BorderMode.Reflect)
+    got = o.tensor().float().cpu().numpy().astype(np.float64)
+    ref = O.compose_total(v.float().cpu().numpy().astype(np.float64),
+                          [(ax, O.gaussian_weights(sg)) for ax, sg in enumerate(sig) if sg > 0], O.REFLECT)
+    rel = np.abs(got - ref) / np.maximum(np.abs(ref), 1e-30)
+    return {"max_rel": float("%.3g" % rel.max()), "rms_rel": float("%.3g" % np.sqrt((rel ** 2).mean())),
+            "sample": "96x3x128x128 crop, same distribution, vs FP64 oracle"}
+
+
 def other_forms(args, hbm):
     """The other BASELINE configurations, timed briefly (each > L2)."""
     import torch
@@ -403,6 +430,17 @@ def other_forms(args, hbm):
                                         "frac_of_measured_hbm": round(2.0 * vox / ms / 1e6 / hbm, 4),
                                         "exact": "bit-exact integer path"}
     del base, src, dst
+    # gradient (convolution.h:359-388): 256^3 f32 -> {3, 256^3} central
+    # differences, Reflect; 16 algorithmic bytes per voxel (read 4, write 12)
+    x = torch.randn((256, 256, 256), generator=g, device="cuda")
+    s = Image.from_tensor(x)
+    o = Image.empty([3, 256, 256, 256], torch.float32)
+    ms = time_call(lambda: n.gradient(s, o, BorderMode.Reflect), it)
+    vox = x.numel()
+    out["gradient_f32_256^3"] = {"ms": round(ms, 4), "gvoxel_s": round(vox / ms / 1e6, 2),
+                                 "gbs": round(16.0 * vox / ms / 1e6, 1),
+                                 "frac_of_measured_hbm": round(16.0 * vox / ms / 1e6 / hbm, 4)}
+    del x, s, o
     # config 5: 4-D video 1024x1024x3x96, sigma (2.5, 2.5, -, 1.5), Reflect
     for name, dt in (("video_bf16", torch.bfloat16), ("video_f16", torch.float16), ("video_f32", torch.float32)):
         v = torch.rand((96, 3, 1024, 1024), generator=g, device="cuda", dtype=torch.float32)
@@ -417,6 +455,7 @@ def other_forms(args, hbm):
         out[name] = {"ms": round(ms, 3), "gvoxel_s": round(vox / ms / 1e6, 2), "gbs": round(2.0 * es * vox / ms / 1e6, 1),
                      "frac_of_measured_hbm": round(2.0 * es * vox / ms / 1e6 / hbm, 4)}
         del v, s, o, salt
+        out[name]["error_vs_fp64"] = video_error(dt)
     # config 4: 512 uneven instances, one persistent launch (graph replay),
     # FP32 and BF16 storage, forward and adjoint; against the plain per-call
     # FP32 path on the same instances

@@ -139,6 +139,14 @@ NDLGPU_API ndlgpu_status ndlgpu_convolve_ex(const ndlgpu_view* src, const ndlgpu
                                  const ndlgpu_view* kernel, int border, int precision,
                                  void* stream);
 
+/* ndl::gradient(src, dst, border)  -- processing/convolution.h:359-388.
+ * dst has rank(src) + 1 axes, a leading component axis of extent rank(src)
+ * and then src's extents ({DIM, ...}); dst.slice(0, a) receives the central
+ * difference along axis a, i.e. convolve() with the {-0.5, 0, +0.5} taps
+ * along that axis (zero centre tap skipped, truncation for integral DstT).
+ * The reference's default border is Reflect. */
+NDLGPU_API ndlgpu_status ndlgpu_gradient(const ndlgpu_view* src, const ndlgpu_view* dst, int border, void* stream);
+
 /* ndl::gaussian_blur(src, dst, sigma, border) -- processing/convolution.h:107-186.
  * Radius ceil(3*sigma) (mathHelpers.h:17-18), weights exp(-d^2/(2 sigma^2))
  * normalised in double on the host (convolution.h:116-126), one pass per

@@ -11,8 +11,11 @@
  *   template<class SrcImageT, class DstImageT>
  *   void ndl::gaussian_blur(const SrcImageT&, DstImageT&, double sigma, BorderMode = Clamp);
  *                                                   -- processing/convolution.h:107-108
+ *   template<class SrcImageT, class DstImageT>
+ *   void ndl::gradient(const SrcImageT&, DstImageT&, BorderMode = Reflect);
+ *                                                   -- processing/convolution.h:359-360
  *
- * ndlgpu::convolve / ndlgpu::gaussian_blur take the same arguments (plus an
+ * ndlgpu::convolve / ndlgpu::gaussian_blur / ndlgpu::gradient take the same arguments (plus an
  * optional CUDA stream) where src and dst are views of DEVICE memory: any type
  * with extent(), stride() and at() returning a reference -- an ndl::Image<T,DIM>
  * constructed over a device pointer, or any view derived from it by
@@ -107,6 +110,17 @@ void convolve(const SrcImageT& src, DstImageT& dst, const KernelT& kernel, Borde
     const ndlgpu_view d = detail::view_of(dst);
     const ndlgpu_view k = detail::view_of(kernel);   // host memory
     detail::check(ndlgpu_convolve(&s, &d, &k, static_cast<int>(border), stream));
+}
+
+/// ndl::gradient on device memory (processing/convolution.h:359-388): dst has
+/// a leading component axis of extent DIM; dst.slice(0, a) gets the central
+/// difference along axis a.  The reference's default border is Reflect (2).
+template <class SrcImageT, class DstImageT, class BorderT = int>
+void gradient(const SrcImageT& src, DstImageT& dst, BorderT border = BorderT(NDLGPU_REFLECT), void* stream = nullptr)
+{
+    const ndlgpu_view s = detail::view_of(src);
+    const ndlgpu_view d = detail::view_of(dst);
+    detail::check(ndlgpu_gradient(&s, &d, static_cast<int>(border), stream));
 }
 
 /// ndl::gaussian_blur on device memory (processing/convolution.h:107-186).

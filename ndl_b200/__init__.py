@@ -6,7 +6,7 @@ of include/ndlgpu.h); this package is its Python host mirror.
 """
 from . import abi
 from .abi import NdlGpuError
-from .convolution import (convolve, convolve_axes, convolve_axes_adjoint, convolve_axes_workspace_size,
+from .convolution import (convolve, gradient, convolve_axes, convolve_axes_adjoint, convolve_axes_workspace_size,
                           gaussian_blur, gaussian_blur_axes, gaussian_radius, gaussian_taps)
 from .image import BorderMode, Image
 

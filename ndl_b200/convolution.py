@@ -58,6 +58,20 @@ def _host_kernel_view(kernel, rank):
     return abi.make_view(k.ctypes.data, code, ext, st), k
 
 
+def gradient(src: Image, dst: Image = None, border=BorderMode.Reflect, stream=None):
+    """ndl::gradient(src, dst, border): dst.slice(0, a) is the central
+    difference along axis a, i.e. convolve() with the taps {-0.5, 0, +0.5}
+    along a (processing/convolution.h:359-388).  dst has a leading component
+    axis of extent src.dim followed by src's extents; with dst None one is
+    made in src's type.  The reference's default border is Reflect."""
+    if dst is None:
+        dst = Image.empty([src.dim] + list(src.extent()), src.dtype)
+    lib = abi.load()
+    sv, dv = src.abi_view(), dst.abi_view()
+    abi.check(lib.ndlgpu_gradient(ctypes.byref(sv), ctypes.byref(dv), int(border), _stream_ptr(stream)))
+    return dst
+
+
 def convolve(src: Image, dst: Image, kernel, border=BorderMode.Clamp, precision=abi.PREC_AUTO, stream=None):
     """ndl::convolve(src, dst, kernel, border): correlation (kernel not
     flipped), centred at K/2 per axis, zero taps skipped, border-mapped per

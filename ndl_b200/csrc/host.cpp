@@ -1283,7 +1283,7 @@ static ndlgpu_status batch_add(BatchHost* b, const ndlgpu_view* src, const ndlgp
         const int B = batch_bucket(K);
         if (B < 0 || K > kBatchMaxTaps) return fail(NDLGPU_ERR_TOO_MANY_TAPS, "batched passes have at most 37 taps");
         if (K / 2 > a.n && border != NDLGPU_CLAMP)
-            return fail(NDLGPU_ERR_INVALID_ARGUMENT, "a Wrap/Reflect pass's radius exceeds its axis extent");
+            return fail(NDLGPU_ERR_RADIUS_EXCEEDS_EXTENT, "a Wrap/Reflect pass's radius exceeds its axis extent");
         has_pass[r] = true;
         *bb[r] = B;
         *rr[r] = K / 2;
@@ -1647,6 +1647,47 @@ ndlgpu_status ndlgpu_convolve_ex(const ndlgpu_view* src, const ndlgpu_view* dst,
     if (e != cudaSuccess) return cuda_fail(e, "N-D kernel");
     // the pageable-memory copies above completed staging before returning;
     // the scratch is released stream-ordered after the kernel
+    return NDLGPU_OK;
+}
+
+ndlgpu_status ndlgpu_gradient(const ndlgpu_view* src, const ndlgpu_view* dst, int border, void* stream)
+{
+    // ndl::gradient (processing/convolution.h:359-388): for every axis a,
+    // convolve(src, dst.slice(0, a), kernel {-0.5, 0, +0.5} along a)
+    t_last_error.clear();
+    ndlgpu_status st;
+    if ((st = check_view(src, "src", true)) != NDLGPU_OK) return st;
+    if ((st = check_view(dst, "dst", true)) != NDLGPU_OK) return st;
+    if (border < NDLGPU_CLAMP || border > NDLGPU_REFLECT) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "unknown border mode");
+    const int R = src->rank;
+    if (dst->rank != R + 1)
+        return fail(NDLGPU_ERR_INVALID_ARGUMENT, "gradient dst must have one more axis than src (a leading component axis)");
+    if (dst->extent[0] != R) return fail(NDLGPU_ERR_EXTENT_MISMATCH, "gradient dst's leading extent must equal src's rank");
+    for (int d = 0; d < R; d++)
+        if (dst->extent[d + 1] != src->extent[d])
+            return fail(NDLGPU_ERR_EXTENT_MISMATCH, "gradient dst's extents after the first must equal src's");
+    if (view_count(src) == 0) return NDLGPU_OK;
+    for (int a = 0; a < R; a++) {
+        ndlgpu_view slice{};
+        slice.data = static_cast<char*>(dst->data) + (ptrdiff_t)a * dst->stride[0] * dtype_size(dst->dtype);
+        slice.dtype = dst->dtype;
+        slice.rank = R;
+        for (int d = 0; d < R; d++) {
+            slice.extent[d] = dst->extent[d + 1];
+            slice.stride[d] = dst->stride[d + 1];
+        }
+        if ((st = check_pair(src, &slice)) != NDLGPU_OK) return st;
+        LPass lp;
+        lp.axis = a;
+        lp.center = 1;
+        lp.taps = {-0.5, 0.0, 0.5};
+        Canon c;
+        Plan pl;
+        st = prepare(src, &slice, {lp}, border, NDLGPU_CAST_EACH, NDLGPU_PREC_AUTO, &c, &pl);
+        if (st != NDLGPU_OK) return st;
+        if (c.total == 0) continue;
+        if ((st = execute(c, pl, NDLGPU_CAST_EACH, border, nullptr, 0, (cudaStream_t)stream)) != NDLGPU_OK) return st;
+    }
     return NDLGPU_OK;
 }
 

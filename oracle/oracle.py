@@ -81,7 +81,7 @@ def _load_ref():
         if not have_reference():
             raise RuntimeError("reference shim not built (oracle/build_oracle.py needs the ndl source tree)")
         _ref = ctypes.CDLL(reference_path())
-        for name in ("ref_convolve", "ref_gaussian_blur", "ref_compose", "ref_view_probe"):
+        for name in ("ref_convolve", "ref_gaussian_blur", "ref_compose", "ref_view_probe", "ref_gradient"):
             getattr(_ref, name).restype = ctypes.c_int
     return _ref
 
@@ -214,6 +214,25 @@ def cast(total, out_code, mode=STORE_CAST):
     return out
 
 
+def gradient(src, border=REFLECT, out_code=None, code=None):
+    """ndl::gradient (processing/convolution.h:359-388) restated: for every
+    ndl axis a, convolve() with the taps {-0.5, 0, +0.5} along a, cast as
+    convolve() casts (truncating for integral DstT).  Returns src.shape +
+    (DIM,): the leading ndl component axis is the last numpy axis."""
+    code = dtype_code(src, code)
+    out_code = code if out_code is None else out_code
+    x = to_f64(src, code)
+    dim = x.ndim
+    comps = []
+    for a in range(dim):
+        kshape = [1] * dim
+        kshape[dim - 1 - a] = 3
+        k = np.zeros(kshape)
+        k.flat[0], k.flat[2] = -0.5, 0.5
+        comps.append(cast(convolve_total(x, k, border), out_code, STORE_CAST))
+    return np.stack(comps, axis=-1)
+
+
 def compose(src, passes, border=CLAMP, out_code=F32, mode=STORE_ROUND, code=None):
     """Oracle of a per-axis separable composition.
 
@@ -294,6 +313,19 @@ def ref_convolve(src, kernel, border=CLAMP, out_dtype=None, out=None):
                           k.ctypes.data_as(_f64p), _i32arr(list(k.shape[::-1])), border)
     if rc != 0:
         raise RuntimeError("ref_convolve failed (%d)" % rc)
+    return out
+
+
+def ref_gradient(src, border=REFLECT, out_dtype=None):
+    """Runs ndl::gradient() itself; returns src.shape + (DIM,)."""
+    lib = _load_ref()
+    out = np.zeros(src.shape + (src.ndim,), out_dtype or src.dtype)
+    ext, sst = _ndl_geom(src)
+    _, dst = _ndl_geom(out)
+    rc = lib.ref_gradient(src.ndim, dtype_code(src), ctypes.c_void_p(src.ctypes.data), _i32arr(ext), _i32arr(sst),
+                          dtype_code(out), ctypes.c_void_p(out.ctypes.data), _i32arr(dst), border)
+    if rc != 0:
+        raise RuntimeError("ref_gradient failed (%d)" % rc)
     return out
 
 

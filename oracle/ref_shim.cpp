@@ -39,6 +39,21 @@ struct StridedView {
         return p[o];
     }
     std::vector<std::array<int, DIM>> coordinates() const { return ndl::detail::coordinatesOf(ext); }
+    // the rank-(DIM-1) view at `index` along axis d, as Image::slice()
+    // builds it (image/core.h:709-712, :814-823); ndl::gradient() uses it
+    template <int D = DIM, std::enable_if_t<(D > 1), int> = 0>
+    StridedView<T, DIM - 1> slice(int d, int index) const
+    {
+        StridedView<T, DIM - 1> v;
+        v.p = p + (long long)index * str[d];
+        for (int i = 0, j = 0; i < DIM; i++) {
+            if (i == d) continue;
+            v.ext[j] = ext[i];
+            v.str[j] = str[i];
+            j++;
+        }
+        return v;
+    }
 };
 
 template <class T, int DIM>
@@ -103,6 +118,29 @@ ndl::Image<double, DIM> axis_kernel(int axis, int K, const double* w, std::vecto
 }  // namespace
 
 extern "C" {
+
+// ndl::gradient(src, dst, border) (processing/convolution.h:359-388): dst of
+// extent {dim, ext...} with strides dstr[0..dim].
+int ref_gradient(int dim, int tsrc, void* src, const int* ext, const int* sstr, int tdst, void* dst, const int* dstr,
+                 int border)
+{
+    return dispatch_dim(dim, [&](auto D) {
+        constexpr int DIM = decltype(D)::value;
+        return dispatch_type(tsrc, [&](auto s) {
+            using S = decltype(s);
+            return dispatch_type(tdst, [&](auto d) {
+                using Dt = decltype(d);
+                auto sv = make_view<S, DIM>(src, ext, sstr);
+                int dext[DIM + 1];
+                dext[0] = DIM;
+                for (int i = 0; i < DIM; i++) dext[i + 1] = ext[i];
+                auto dv = make_view<Dt, DIM + 1>(dst, dext, dstr);
+                ndl::gradient(sv, dv, to_border(border));
+                return 0;
+            });
+        });
+    });
+}
 
 // ndl::convolve(src, dst, kernel, border) on arbitrary strided views; kernel
 // is a contiguous double array of extent kext (axis 0 fastest).

@@ -94,7 +94,51 @@ int main()
         }
         cudaFree(db);
     }
-    // 3. the reference asserts on mismatched extents; the drop-in throws
+    // 3. gradient (default border Reflect) of a float view and of uint8 into
+    //    int16, against ndl::gradient itself, bit-exact
+    {
+        const int NX = 40, NY = 33, NZ = 27;
+        std::vector<float> fb((size_t)NX * NY * NZ);
+        std::normal_distribution<float> nd(0.f, 1.f);
+        for (auto& v : fb) v = nd(rng);
+        ndl::Image<float, 3> hf(fb.data(), {NX, NY, NZ});
+        auto hv = hf.swap_axes(0, 2).mirror(1);
+        float* df = upload(fb);
+        ndl::Image<float, 3> gf(df, {NX, NY, NZ});
+        auto gv = gf.swap_axes(0, 2).mirror(1);
+        const auto e3 = hv.extent();
+        ndl::OwnedImage<float, 4> ref({3, e3[0], e3[1], e3[2]});
+        ndl::gradient(hv, ref);
+        std::vector<float> got((size_t)3 * NX * NY * NZ, 0.f);
+        float* dg = upload(got);
+        ndl::Image<float, 4> gg(dg, {3, e3[0], e3[1], e3[2]});
+        ndlgpu::gradient(gv, gg);
+        cudaMemcpy(got.data(), dg, got.size() * sizeof(float), cudaMemcpyDeviceToHost);
+        size_t bad = 0, i = 0;
+        for (const auto& c : ref.coordinates()) bad += (got[i++] != ref.at(c));
+        report("gradient f32 view swap_axes(0,2).mirror(1), bit-exact", bad == 0, (double)bad);
+        std::vector<uint8_t> ub((size_t)NX * NY * NZ);
+        for (auto& v : ub) v = (uint8_t)(rng() & 255);
+        ndl::Image<uint8_t, 3> hu(ub.data(), {NX, NY, NZ});
+        uint8_t* du = upload(ub);
+        ndl::Image<uint8_t, 3> gu(du, {NX, NY, NZ});
+        ndl::OwnedImage<int16_t, 4> ref16({3, NX, NY, NZ});
+        ndl::gradient(hu, ref16, ndl::BorderMode::Clamp);
+        std::vector<int16_t> got16((size_t)3 * NX * NY * NZ, 0);
+        int16_t* d16 = upload(got16);
+        ndl::Image<int16_t, 4> g16(d16, {3, NX, NY, NZ});
+        ndlgpu::gradient(gu, g16, ndl::BorderMode::Clamp);
+        cudaMemcpy(got16.data(), d16, got16.size() * sizeof(int16_t), cudaMemcpyDeviceToHost);
+        bad = 0;
+        i = 0;
+        for (const auto& c : ref16.coordinates()) bad += (got16[i++] != ref16.at(c));
+        report("gradient u8 -> int16 Clamp (truncation), bit-exact", bad == 0, (double)bad);
+        cudaFree(df);
+        cudaFree(dg);
+        cudaFree(du);
+        cudaFree(d16);
+    }
+    // 4. the reference asserts on mismatched extents; the drop-in throws
     {
         float* d = nullptr;
         cudaMalloc(&d, 64 * sizeof(float));

@@ -183,3 +183,19 @@ def test_oracle_matches_compiled_reference_random(seed):
         sig = float(rng.uniform(0.4, 1.2))
         if b == O.CLAMP or 2 * O.gaussian_radius(sig) < min(shape):
             assert (O.ref_gaussian_blur(x, sig, b) == O.gaussian_blur(x, sig, b)).all()
+
+
+@pytest.mark.skipif(not O.have_reference(), reason="compiled reference not present")
+@pytest.mark.parametrize("shape", [(17,), (9, 13), (5, 7, 11)])
+def test_gradient_oracle_matches_compiled_reference(shape):
+    """The oracle's gradient() (convolve with {-0.5, 0, +0.5} per axis, cast
+    as convolve casts) against ndl::gradient() itself, bit for bit."""
+    rng = np.random.default_rng(len(shape))
+    for dt, odt in [(np.float32, np.float32), (np.uint8, np.int16), (np.int32, np.int32), (np.float64, np.float64),
+                    (np.uint8, np.float32)]:
+        x = rng.standard_normal(shape).astype(dt) if dt in (np.float32, np.float64) else \
+            (rng.random(shape) * 200).astype(dt)
+        for border in (0, 1, 2):
+            r = O.ref_gradient(x, border, odt)
+            o = O.gradient(x, border, O.dtype_code(np.zeros(1, odt)))
+            assert (r == o).all(), (dt, odt, border)
