@@ -1677,6 +1677,38 @@ ndlgpu_status ndlgpu_gradient(const ndlgpu_view* src, const ndlgpu_view* dst, in
             slice.stride[d] = dst->stride[d + 1];
         }
         if ((st = check_pair(src, &slice)) != NDLGPU_OK) return st;
+    }
+    // one pass over the source for ranks 1..3 (gradient.cu)
+    GradParams gp{};
+    gp.src = static_cast<const char*>(src->data);
+    gp.dst = static_cast<char*>(dst->data);
+    gp.sdt = src->dtype;
+    gp.ddt = dst->dtype;
+    gp.rank = R;
+    gp.border = border;
+    bool fits = R <= 3;
+    for (int d = 0; d < R && fits; d++) {
+        if (src->extent[d] > 0x7fffffffLL) fits = false;
+        gp.ext[d] = (int)src->extent[d];
+        gp.sstr[d] = src->stride[d];
+        gp.dstr[d + 1] = dst->stride[d + 1];
+    }
+    gp.dstr[0] = dst->stride[0];
+    if (fits && gradient_supported(gp)) {
+        cudaError_t e = launch_gradient(gp, (cudaStream_t)stream);
+        return e == cudaSuccess ? NDLGPU_OK : cuda_fail(e, "gradient launch");
+    }
+    // any rank: one convolve() pass per axis, as the reference runs it
+    for (int a = 0; a < R; a++) {
+        ndlgpu_view slice{};
+        slice.data = static_cast<char*>(dst->data) + (ptrdiff_t)a * dst->stride[0] * dtype_size(dst->dtype);
+        slice.dtype = dst->dtype;
+        slice.rank = R;
+        for (int d = 0; d < R; d++) {
+            slice.extent[d] = dst->extent[d + 1];
+            slice.stride[d] = dst->stride[d + 1];
+        }
+        if ((st = check_pair(src, &slice)) != NDLGPU_OK) return st;
         LPass lp;
         lp.axis = a;
         lp.center = 1;

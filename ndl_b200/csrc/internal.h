@@ -242,6 +242,20 @@ long long tapgrad_ctas(const TapFusedParams& p);
 int tapgrad_zchunk(int nx, int ny, int nz, int nbatch, int kz);
 cudaError_t launch_tapgrad(const TapFusedParams& p, void* out, int out_dtype, const TapFinalMap& mp, cudaStream_t s);
 
+// gradient (gradient.cu): all DIM central differences of a voxel in one pass.
+struct GradParams {
+    const char* src;
+    char* dst;
+    int sdt, ddt;
+    int rank;                 // 1..3
+    int border;
+    int ext[3];
+    int64_t sstr[3];          // source strides, elements
+    int64_t dstr[4];          // destination strides: [0] the component axis
+};
+bool gradient_supported(const GradParams& p);
+cudaError_t launch_gradient(const GradParams& p, cudaStream_t s);
+
 // Batched form (batch.cu): one persistent launch over a table of instances.
 constexpr int kBatchMaxTaps = 37;
 struct BatchDesc {

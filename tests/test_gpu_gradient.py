@@ -21,7 +21,7 @@ def ndl_dst(src, dtype):
     return Image.empty([src.dim] + src.extent(), dtype)
 
 
-@pytest.mark.parametrize("shape", [(300,), (37, 41), (19, 23, 29), (4, 64, 64, 64)])
+@pytest.mark.parametrize("shape", [(300,), (37, 41), (40, 64), (19, 23, 29), (16, 24, 32), (4, 64, 64, 64)])
 @pytest.mark.parametrize("border", [0, 1, 2])
 @pytest.mark.parametrize("dt,odt", [(np.float32, np.float32), (np.uint8, np.int16), (np.int32, np.int32),
                                     (np.float64, np.float64), (np.uint8, np.float32)])
