@@ -17,7 +17,20 @@
 //           dispatch so that no value is ever moved.
 // Border maps are Clamp / Wrap / Reflect of mathHelpers.h:23-25, applied to
 // load coordinates only.
+//
+// The adjoint with Clamp/Reflect reads zero outside the image.  Where the
+// source rows are 16-byte aligned, its planes come in through the copy engine
+// instead: one 4-D tensor-map box (cp.async.bulk.tensor) per plane, issued by
+// one thread and completed on an mbarrier; the engine's out-of-bounds zero
+// fill is exactly that zero padding, so no element-copy table is needed.
+// Every mbarrier wait is bounded: on timeout the CTA sets bit 1 of the guard
+// word and returns.
+#include <algorithm>
+#include <cstring>
 #include <utility>
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
 
 #include "dtype.cuh"
 
@@ -92,6 +105,45 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
+__device__ int32_t g_guard_fused;
+
+constexpr int kTmaSpins = 1 << 22;   // bound on the mbarrier polls for one plane
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// orders this thread's earlier generic-proxy shared-memory accesses before
+// the copy engine's writes that it issues next
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+// one box of a 4-D tensor map into shared memory, completing on bar
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1, int c2,
+                                            int c3)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, "
+        "%6}], [%2];\n" ::"r"(smem_u32(dst)),
+        "l"(map), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+        : "memory");
+}
+
 template <class Tin, int KX, int KY, int TY_>
 struct Geo {
     static constexpr int TY = TY_;
@@ -111,12 +163,14 @@ struct Geo {
     static constexpr int PITCH = (NCH * EPC > WEND ? NCH * EPC : (WEND + EPC - 1) / EPC * EPC);
     static constexpr int NTASK = (ROWS * NCH + NT - 1) / NT;
     static constexpr int NXU = (ROWS * 16 + NT - 1) / NT;       // X-pass units per thread
-    static constexpr size_t IN_BYTES = (size_t)STAGES * ROWS * PITCH * sizeof(Tin);
+    static constexpr size_t STAGE_BYTES = (size_t)ROWS * PITCH * sizeof(Tin);
+    static constexpr size_t IN_BYTES = (size_t)STAGES * STAGE_BYTES;
     static constexpr size_t X_BYTES = (size_t)ROWS * TX * sizeof(float);
     // element-copy table: border columns and ragged chunks, built once per CTA
     static constexpr int MAXEL = ROWS * PITCH;
     static constexpr size_t TAB_BYTES = (size_t)MAXEL * 8;
-    static constexpr size_t SMEM = IN_BYTES + X_BYTES + TAB_BYTES + 16;
+    static constexpr size_t SMEM = IN_BYTES + X_BYTES + TAB_BYTES + 16 + 128;   // + alignment slack
+    static_assert(STAGE_BYTES % 128 == 0, "plane stages stay 128-byte aligned for the copy engine");
 };
 
 // Output plane sum of the Z queue for the newest slot S: tap k reads slot
@@ -173,12 +227,17 @@ struct Occ {
     static constexpr int value = TY <= 16 ? ((ADJ && KZ > 9) ? 3 : 4) : 2;
 };
 
-template <class Tin, class Tout, int KX, int KY, int KZ, int TY, bool ADJ>
-__global__ void __launch_bounds__(8 * TY, (Occ<TY, ADJ, KZ>::value)) k_fused2(const __grid_constant__ FusedParams p)
+// TMA: plane loads through the tensor map (adjoint with zero padding only).
+template <class Tin, class Tout, int KX, int KY, int KZ, int TY, bool ADJ, bool TMA>
+__global__ void __launch_bounds__(8 * TY, (Occ<TY, ADJ, KZ>::value))
+    k_fused2(const __grid_constant__ FusedParams p, const __grid_constant__ CUtensorMap tmap)
 {
     using G = Geo<Tin, KX, KY, TY>;
     constexpr int NT = G::NT;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    static_assert(!TMA || ADJ, "the copy-engine loader serves the zero-padded adjoint");
+    extern __shared__ __align__(128) unsigned char smem_dyn[];
+    __shared__ uint64_t s_bar[STAGES];
+    unsigned char* smem_raw = smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);
     Tin* s_in = reinterpret_cast<Tin*>(smem_raw);
     float* s_x = reinterpret_cast<float*>(smem_raw + G::IN_BYTES);
     int2* s_tab = reinterpret_cast<int2*>(smem_raw + G::IN_BYTES + G::X_BYTES);
@@ -207,7 +266,13 @@ __global__ void __launch_bounds__(8 * TY, (Occ<TY, ADJ, KZ>::value)) k_fused2(co
     // registers); every other element goes to a shared table of (shared
     // offset, in-plane global offset) pairs with its column border-mapped.
     const bool zp = ADJ && p.zero_pad;   // adjoint, Clamp/Reflect: zero outside the image
-    if (tid == 0) *s_ntab = 0;
+    if (tid == 0) {
+        *s_ntab = 0;
+        if constexpr (TMA) {
+            for (int st = 0; st < STAGES; st++) mbar_init(&s_bar[st], 1);
+            fence_mbar_init();
+        }
+    }
     __syncthreads();
     int32_t goff[G::NTASK];
     int32_t soff[G::NTASK];
@@ -216,6 +281,7 @@ __global__ void __launch_bounds__(8 * TY, (Occ<TY, ADJ, KZ>::value)) k_fused2(co
         const int t = tid + j * NT;
         goff[j] = -1;
         soff[j] = 0;
+        if constexpr (TMA) continue;
         if (t >= G::ROWS * G::NCH) continue;
         const int r = t / G::NCH;
         const int q = t - r * G::NCH;
@@ -250,6 +316,18 @@ __global__ void __launch_bounds__(8 * TY, (Occ<TY, ADJ, KZ>::value)) k_fused2(co
 
     auto issue = [&](int zi, int stage) {
         Tin* sb = s_in + stage * (G::ROWS * G::PITCH);
+        if constexpr (TMA) {
+            // one box: rows y0-CY.., columns gx0.. of plane zi; the planes,
+            // rows and columns outside the image come back zero-filled
+            if (tid == 0) {
+                const int yc = y0 - G::CY;
+                auto coord = [&](int d) { return p.tma_pos[0] == d ? yc : (p.tma_pos[1] == d ? zi : bat); };
+                fence_proxy_async();
+                mbar_expect_tx(&s_bar[stage], (unsigned)G::STAGE_BYTES);
+                tma_load_4d(sb, &tmap, &s_bar[stage], gx0, coord(0), coord(1), coord(2));
+            }
+            return;
+        }
         if (zp && (zi < 0 || zi >= p.nz)) {
             // a plane outside the image: zero what the copies would fill
 #pragma unroll
@@ -297,6 +375,7 @@ __global__ void __launch_bounds__(8 * TY, (Occ<TY, ADJ, KZ>::value)) k_fused2(co
     const bool yzone = ey[0] >= 0 || ey[1] >= 0;
     const bool xzone_tile = zp && (x0 < G::CX || x0 + TX > p.nx - G::CX);
     int slot = 0;
+    unsigned phase = 0;                  // mbarrier parity of the current pass over the ring
     int stage = 0;                       // ring stage of plane n
     int stage_next = STAGES - 1;         // ring stage of plane n + STAGES - 1
     // output rows of this thread: row offsets and, per plane, a running
@@ -307,8 +386,19 @@ __global__ void __launch_bounds__(8 * TY, (Occ<TY, ADJ, KZ>::value)) k_fused2(co
     for (int h = 0; h < 2; h++) rowoff[h] = (int64_t)(y0 + 2 * gy + h) * p.dy;
     Tout* oplane = dst + (int64_t)(zin0 + KZ - 1 - HZ) * p.dz;
     for (int n = 0; n < nplanes; n++) {
-        cp_async_wait<STAGES - 2>();
-        __syncthreads();    // plane n visible; every thread is past the X pass of plane n-1
+        if constexpr (TMA) {
+            bool ok = false;
+            for (int i = 0; i < kTmaSpins && !ok; i++) ok = mbar_try_wait(&s_bar[stage], phase);
+            // plane n visible; every thread is past the X pass of plane n-1
+            if (__syncthreads_or(!ok)) {
+                if (tid == 0) atomicOr(&g_guard_fused, 2);
+                return;
+            }
+            if (stage + 1 == STAGES) phase ^= 1u;
+        } else {
+            cp_async_wait<STAGES - 2>();
+            __syncthreads();    // plane n visible; every thread is past the X pass of plane n-1
+        }
         if (n + STAGES - 1 < nplanes) issue(zin0 + n + STAGES - 1, stage_next);
         cp_async_commit();
         stage_next = (stage_next + 1 == STAGES) ? 0 : stage_next + 1;
@@ -444,16 +534,91 @@ __global__ void __launch_bounds__(8 * TY, (Occ<TY, ADJ, KZ>::value)) k_fused2(co
 
 using LaunchFn = cudaError_t (*)(const FusedParams&, cudaStream_t);
 
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    }();
+    return fn;
+}
+
+template <class T> constexpr CUtensorMapDataType tma_type();
+template <> constexpr CUtensorMapDataType tma_type<float>() { return CU_TENSOR_MAP_DATA_TYPE_FLOAT32; }
+template <> constexpr CUtensorMapDataType tma_type<__nv_bfloat16>() { return CU_TENSOR_MAP_DATA_TYPE_BFLOAT16; }
+template <> constexpr CUtensorMapDataType tma_type<__half>() { return CU_TENSOR_MAP_DATA_TYPE_FLOAT16; }
+
+// A 4-D tiled map of the source -- x, then y, z and batch in increasing
+// stride order -- with a box of boxx columns x boxy rows of one plane, for
+// the adjoint with Clamp/Reflect (its zero padding is the copy engine's
+// fill); p.tma_pos gets the map dimension (0..2 after x) of y, z and batch.
+// False where the plane loads keep the cp.async path: the forward (a
+// border-mapped halo would have to be rewritten in every border tile), Wrap,
+// unaligned, non-unit-stride or negative-stride sources, or an encode failure.
+template <class Tin>
+bool plane_map(FusedParams& p, int boxx, int boxy, CUtensorMap* m)
+{
+    if (!p.adj || !p.zero_pad || !p.vec_ld || p.sx != 1) return false;
+    if (reinterpret_cast<uintptr_t>(p.src) % 16 != 0) return false;
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return false;
+    const int64_t es = (int64_t)sizeof(Tin);
+    struct Dim {
+        int64_t n, s;
+        int role;
+    } d[3] = {{p.ny, p.sy, 0}, {p.nz, p.sz, 1}, {p.nbatch, p.sb, 2}};
+    int64_t span = es * p.nx;
+    for (const Dim& e : d) {
+        if (e.n <= 1) continue;
+        if (e.s <= 0 || (e.s * es) % 16 != 0) return false;
+        span = std::max(span, e.s * es * e.n);
+    }
+    span = (span + 15) / 16 * 16;
+    for (Dim& e : d)
+        if (e.n <= 1) e.s = span / es;   // never stepped: any valid stride
+    std::stable_sort(d, d + 3, [](const Dim& a, const Dim& b) { return a.s < b.s; });
+    cuuint64_t gdim[4] = {(cuuint64_t)p.nx, 0, 0, 0};
+    cuuint64_t gstr[3];
+    cuuint32_t box[4] = {(cuuint32_t)boxx, 1, 1, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    for (int i = 0; i < 3; i++) {
+        gdim[i + 1] = (cuuint64_t)d[i].n;
+        gstr[i] = (cuuint64_t)(d[i].s * es);
+        if (gstr[i] >= (1ull << 40)) return false;
+        p.tma_pos[d[i].role] = i;
+        if (d[i].role == 0) box[i + 1] = (cuuint32_t)boxy;
+    }
+    std::memset(m, 0, sizeof(*m));
+    const CUresult r = enc(m, tma_type<Tin>(), 4, const_cast<char*>(p.src), gdim, gstr, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
 template <class Tin, class Tout, int KX, int KY, int KZ, int TY, bool ADJ>
 cudaError_t launch2(const FusedParams& p, cudaStream_t s)
 {
     using G = Geo<Tin, KX, KY, TY>;
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(k_fused2<Tin, Tout, KX, KY, KZ, TY, ADJ>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM);
+    static_assert(G::PITCH <= 256 && G::ROWS <= 256, "tensor-map boxes hold at most 256 per dimension");
+    static_assert(G::PITCH * sizeof(Tin) % 16 == 0, "box rows are whole 16-byte units");
+    static bool configured[2] = {false, false};
+    FusedParams pp = p;
+    CUtensorMap tmap;
+    std::memset(&tmap, 0, sizeof(tmap));
+    bool tma = false;
+    auto kern = k_fused2<Tin, Tout, KX, KY, KZ, TY, ADJ, false>;
+    if constexpr (ADJ) {
+        tma = plane_map<Tin>(pp, G::PITCH, G::ROWS, &tmap);
+        if (tma) kern = k_fused2<Tin, Tout, KX, KY, KZ, TY, ADJ, true>;
+    }
+    if (!configured[tma]) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM);
         if (e != cudaSuccess) return e;
-        configured = true;
+        configured[tma] = true;
     }
     const int ntx = (p.nx + TX - 1) / TX;
     const int nty = (p.ny + TY - 1) / TY;
@@ -464,11 +629,10 @@ cudaError_t launch2(const FusedParams& p, cudaStream_t s)
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const long long slots = (long long)sms * Occ<TY, ADJ, KZ>::value;
     const int chunks = pick_zchunks(gx, slots, p.nz, KZ - 1);
-    FusedParams pp = p;
     pp.zchunk = max(1, (p.nz + chunks - 1) / chunks);
     const int gz = (p.nz + pp.zchunk - 1) / pp.zchunk;
     if (gx > 0x7fffffffLL || gz > 65535) return cudaErrorInvalidConfiguration;
-    k_fused2<Tin, Tout, KX, KY, KZ, TY, ADJ><<<dim3((unsigned)gx, (unsigned)gz), G::NT, G::SMEM, s>>>(pp);
+    kern<<<dim3((unsigned)gx, (unsigned)gz), G::NT, G::SMEM, s>>>(pp, tmap);
     count_launch();
     return cudaGetLastError();
 }
@@ -501,6 +665,14 @@ bool fused2_supported(int sdt, int ddt, int kx, int ky, int kz, int adj)
     for (const Variant2& v : kVariants2)
         if (v.adj == adj && v.sdt == sdt && v.ddt == ddt && v.kx == kx && v.ky == ky && v.kz == kz) return true;
     return false;
+}
+
+cudaError_t read_guard_fused(int32_t* v)
+{
+    int32_t zero = 0;
+    cudaError_t e = cudaMemcpyFromSymbol(v, g_guard_fused, sizeof(int32_t));
+    if (e != cudaSuccess) return e;
+    return cudaMemcpyToSymbol(g_guard_fused, &zero, sizeof(int32_t));
 }
 
 cudaError_t launch_fused2(const FusedParams& p, cudaStream_t s)

@@ -182,5 +182,13 @@ cudaError_t read_guard_generic(int32_t* v)
 }  // namespace ndlgpu
 
 namespace ndlgpu {
-cudaError_t read_device_status(cudaStream_t, int32_t* code) { return read_guard_generic(code); }
+cudaError_t read_device_status(cudaStream_t, int32_t* code)
+{
+    int32_t a = 0, b = 0;
+    cudaError_t e = read_guard_generic(&a);
+    if (e != cudaSuccess) return e;
+    e = read_guard_fused(&b);
+    *code = a | b;
+    return e;
+}
 }  // namespace ndlgpu

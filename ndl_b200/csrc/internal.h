@@ -181,6 +181,7 @@ struct FusedParams {
     float wxf[64], wyf[64], wzf[64];
     int32_t wxi[64], wyi[64], wzi[64];
     float2 wx2[40], wy2[40], wz2[40];  // (w, w) pairs of the taps (packed FP32 FMA)
+    int tma_pos[3];       // tensor-map dimension of y, z and batch (set at launch)
 };
 
 // Returns cudaErrorNotSupported when no compiled variant matches.
@@ -189,6 +190,8 @@ bool fused_supported(Acc acc, int src_dtype, int dst_dtype, int kx, int ky, int 
 // Float-storage fused kernel with asynchronous loads (fused2.cu).
 cudaError_t launch_fused2(const FusedParams& p, cudaStream_t s);
 bool fused2_supported(int src_dtype, int dst_dtype, int kx, int ky, int kz, int adj = 0);
+// Reads and clears the fused kernels' guard word (bit 1: a plane load timed out).
+cudaError_t read_guard_fused(int32_t* v);
 
 // Sets the per-thread message ndlgpu_last_error() returns; returns s.
 ndlgpu_status set_error(ndlgpu_status s, const std::string& msg);
