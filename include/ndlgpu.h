@@ -263,8 +263,11 @@ NDLGPU_API ndlgpu_status ndlgpu_gaussian_blur_noalloc(const ndlgpu_view* src, co
 NDLGPU_API uint64_t ndlgpu_kernel_launches(void);
 
 /* ---- device guard word -------------------------------------------------- */
-/* Reads (and clears) the library's device-side guard word on the current
- * device after synchronising `stream`: 0 if no kernel guard fired. */
+/* Reads (and clears) the library's device-side guard words on the current
+ * device after synchronising `stream`: 0 if no kernel guard fired.  Bit 1: a
+ * fused adjoint plane load did not complete within its bounded wait; bit 2: a
+ * batched phase wait ran past its bound (the work item was dropped); other
+ * bits are reserved. */
 NDLGPU_API ndlgpu_status ndlgpu_device_status(void* stream, int32_t* code);
 
 #ifdef __cplusplus

@@ -38,6 +38,8 @@
 namespace ndlgpu {
 namespace {
 
+__device__ int32_t g_guard_batch;   // bit 2: a phase wait ran past its bound
+
 constexpr int kSeg = 128;        // row-pass outputs per warp segment
 constexpr int kColS = 64;        // column-pass outputs per unit along the axis
 constexpr int kMaxSpins = 1 << 22;
@@ -429,6 +431,7 @@ __global__ void __launch_bounds__(256, 3) k_batch(const BatchDesc* __restrict__ 
                     __nanosleep(200);
                     if (++spins > kMaxSpins) {
                         atomicExch(err, 1);
+                        atomicOr(&g_guard_batch, 4);
                         s_skip = 1;
                         break;
                     }
@@ -557,6 +560,14 @@ cudaError_t batch_prepare(int dtype, int cfg, BatchLaunch* L)
     case NDLGPU_F16: return prepare_b<__half>(w, L);
     default: return cudaErrorInvalidValue;
     }
+}
+
+cudaError_t read_guard_batch(int32_t* v)
+{
+    int32_t zero = 0;
+    cudaError_t e = cudaMemcpyFromSymbol(v, g_guard_batch, sizeof(int32_t));
+    if (e != cudaSuccess) return e;
+    return cudaMemcpyToSymbol(g_guard_batch, &zero, sizeof(int32_t));
 }
 
 cudaError_t launch_batch(int dtype, int cfg, const BatchLaunch& L, cudaStream_t s)

@@ -299,6 +299,8 @@ int batch_stage_bytes(int bmax);   // one column-pass stage for the widest taps
 // Sets the kernel attributes and the persistent grid (no stream work).
 cudaError_t batch_prepare(int dtype, int cfg, BatchLaunch* L);
 cudaError_t launch_batch(int dtype, int cfg, const BatchLaunch& L, cudaStream_t s);
+// Reads and clears the batched kernel's guard word (bit 2: a phase wait timed out).
+cudaError_t read_guard_batch(int32_t* v);
 
 // Device guard word.
 cudaError_t read_device_status(cudaStream_t s, int32_t* code);
