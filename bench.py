@@ -406,6 +406,47 @@ def video_error(dt, seed=SEED):
             "sample": "96x3x128x128 crop, same distribution, vs FP64 oracle"}
 
 
+def dog_fma_per_pixel(num_scales, sigma0, tile_rows=32):
+    """FMAs per output pixel of the fused scale-space kernel: each level's X
+    pass covers the tile rows plus that level's halo, then its Y pass."""
+    import ndl_b200 as n
+    total = 0.0
+    for i in range(num_scales):
+        r = n.gaussian_radius(sigma0 * 2.0 ** (i / (num_scales - 3)))
+        total += (2 * r + 1) * ((tile_rows + 2 * r) / tile_rows + 1.0)
+    return total
+
+
+def dog_form(g, it, hbm):
+    """Difference-of-Gaussians scale space (feature_detection.h:101-122) of a
+    4096^2 f32 image, 5 levels from sigma0 = 1.6, Reflect: 20 algorithmic
+    bytes per pixel (read 4, write four 4-byte differences), timed beside the
+    same five levels as five gaussian_blur calls."""
+    import torch
+
+    import ndl_b200 as n
+    from ndl_b200 import BorderMode, Image
+
+    x = torch.rand((4096, 4096), generator=g, device="cuda") * 255.0
+    s = Image.from_tensor(x)
+    dogs = [Image.empty(s.extent(), torch.float32) for _ in range(4)]
+    ms = time_call(lambda: n.dog_scale_space(s, 5, 1.6, dogs=dogs), it)
+    levels = [Image.empty(s.extent(), torch.float32) for _ in range(5)]
+    sig = [1.6 * 2.0 ** (i / 2) for i in range(5)]
+
+    def five_blurs():
+        for i in range(5):
+            n.gaussian_blur(s, levels[i], sig[i], BorderMode.Reflect)
+
+    ms5 = time_call(five_blurs, max(3, it // 4))
+    px = x.numel()
+    fma = dog_fma_per_pixel(5, 1.6)
+    return {"ms": round(ms, 4), "mpix_s": round(px / ms / 1e3, 1), "gbs": round(20.0 * px / ms / 1e6, 1),
+            "frac_of_measured_hbm": round(20.0 * px / ms / 1e6 / hbm, 4),
+            "fp32_tflops": round(2.0 * fma * px / ms / 1e9, 2), "fma_per_pixel": round(fma, 1),
+            "five_gaussian_blur_calls_ms": round(ms5, 4)}
+
+
 def other_forms(args, hbm):
     """The other BASELINE configurations, timed briefly (each > L2)."""
     import torch
@@ -441,6 +482,7 @@ def other_forms(args, hbm):
                                  "gbs": round(16.0 * vox / ms / 1e6, 1),
                                  "frac_of_measured_hbm": round(16.0 * vox / ms / 1e6 / hbm, 4)}
     del x, s, o
+    out["dog_f32_4096^2_5scales"] = dog_form(g, it, hbm)
     # config 5: 4-D video 1024x1024x3x96, sigma (2.5, 2.5, -, 1.5), Reflect
     for name, dt in (("video_bf16", torch.bfloat16), ("video_f16", torch.float16), ("video_f32", torch.float32)):
         v = torch.rand((96, 3, 1024, 1024), generator=g, device="cuda", dtype=torch.float32)

@@ -147,6 +147,21 @@ NDLGPU_API ndlgpu_status ndlgpu_convolve_ex(const ndlgpu_view* src, const ndlgpu
  * The reference's default border is Reflect. */
 NDLGPU_API ndlgpu_status ndlgpu_gradient(const ndlgpu_view* src, const ndlgpu_view* dst, int border, void* stream);
 
+/* The Difference-of-Gaussians scale space of ndl::detect_keypoints
+ * (processing/feature_detection.h:101-122): num_scales (4..64) levels,
+ * level i = gaussian_blur(src as double, sigma_i, Reflect) with
+ * sigma_i = sigma0 * 2^(i / (num_scales - 3)), and num_scales - 1 differences
+ * dogs[i] = level[i+1] - level[i].  `dogs` points to num_scales - 1 views,
+ * `levels` to num_scales views or is NULL; all are F32 or F64 images of src's
+ * extent that overlap neither src nor each other.  2-D images with F32
+ * outputs (up to 16 levels, radius <= 48, sources exact in float) run one
+ * kernel that reads the source once and writes every output (FP32
+ * accumulation); other cases run one blur per level plus a difference pass
+ * (FP64 outputs get the reference's exact double sequence) with
+ * stream-ordered scratch for the levels the caller does not take. */
+NDLGPU_API ndlgpu_status ndlgpu_dog_scale_space(const ndlgpu_view* src, int num_scales, double sigma0,
+                                                const ndlgpu_view* levels, const ndlgpu_view* dogs, void* stream);
+
 /* ndl::gaussian_blur(src, dst, sigma, border) -- processing/convolution.h:107-186.
  * Radius ceil(3*sigma) (mathHelpers.h:17-18), weights exp(-d^2/(2 sigma^2))
  * normalised in double on the host (convolution.h:116-126), one pass per

@@ -72,6 +72,31 @@ def gradient(src: Image, dst: Image = None, border=BorderMode.Reflect, stream=No
     return dst
 
 
+def dog_scale_space(src: Image, num_scales=5, sigma0=1.6, dogs=None, levels=None, dtype=None, stream=None):
+    """The Difference-of-Gaussians scale space of ndl::detect_keypoints
+    (processing/feature_detection.h:101-122): level i is
+    gaussian_blur(src, sigma0 * 2^(i / (num_scales - 3)), Reflect) and
+    dogs[i] = level[i+1] - level[i].  ``dogs`` (num_scales - 1 images) and
+    ``levels`` (num_scales images, or None: not returned) may be given; made
+    ones are contiguous images of ``dtype`` (float32 by default).  Returns
+    (dogs, levels)."""
+    import torch
+    dt = dtype or torch.float32
+    if dogs is None:
+        dogs = [Image.empty(src.extent(), dt) for _ in range(num_scales - 1)]
+    if levels is True:
+        levels = [Image.empty(src.extent(), dt) for _ in range(num_scales)]
+    if len(dogs) != num_scales - 1 or (levels is not None and len(levels) != num_scales):
+        raise ValueError("dog_scale_space needs num_scales - 1 dogs and num_scales levels")
+    lib = abi.load()
+    sv = src.abi_view()
+    dv = (abi.View * len(dogs))(*[d.abi_view() for d in dogs])
+    lv = (abi.View * len(levels))(*[lv.abi_view() for lv in levels]) if levels is not None else None
+    abi.check(lib.ndlgpu_dog_scale_space(ctypes.byref(sv), int(num_scales), ctypes.c_double(sigma0), lv, dv,
+                                         _stream_ptr(stream)))
+    return dogs, levels
+
+
 def convolve(src: Image, dst: Image, kernel, border=BorderMode.Clamp, precision=abi.PREC_AUTO, stream=None):
     """ndl::convolve(src, dst, kernel, border): correlation (kernel not
     flipped), centred at K/2 per axis, zero taps skipped, border-mapped per

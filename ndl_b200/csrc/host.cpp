@@ -1723,6 +1723,163 @@ ndlgpu_status ndlgpu_gradient(const ndlgpu_view* src, const ndlgpu_view* dst, in
     return NDLGPU_OK;
 }
 
+// Blur of one level (gaussian_blur(src, dst, sigma, Reflect)) through the
+// pass-chain planner.
+static ndlgpu_status blur_level(const ndlgpu_view* src, const ndlgpu_view* dst, double sigma, cudaStream_t s)
+{
+    std::vector<LPass> lp;
+    ndlgpu_status st = gaussian_passes(src, &sigma, false, &lp);
+    if (st != NDLGPU_OK) return st;
+    Canon c;
+    Plan pl;
+    st = prepare(src, dst, lp, NDLGPU_REFLECT, NDLGPU_ROUND_ONCE, NDLGPU_PREC_AUTO, &c, &pl);
+    if (st != NDLGPU_OK || c.total == 0) return st;
+    return execute(c, pl, NDLGPU_ROUND_ONCE, NDLGPU_REFLECT, nullptr, 0, s);
+}
+
+// Source types that convert to float exactly (the fused kernel's loads).
+static bool float_exact_dtype(int dt)
+{
+    return dt == NDLGPU_U8 || dt == NDLGPU_I8 || dt == NDLGPU_U16 || dt == NDLGPU_I16 || dt == NDLGPU_F32 ||
+           dt == NDLGPU_F16 || dt == NDLGPU_BF16;
+}
+
+ndlgpu_status ndlgpu_dog_scale_space(const ndlgpu_view* src, int num_scales, double sigma0, const ndlgpu_view* levels,
+                                     const ndlgpu_view* dogs, void* stream)
+{
+    // ndl::detect_keypoints' scale space (processing/feature_detection.h:101-122)
+    t_last_error.clear();
+    ndlgpu_status st;
+    if ((st = check_view(src, "src", true)) != NDLGPU_OK) return st;
+    if (num_scales < 4 || num_scales > kDogMaxScales)
+        return fail(NDLGPU_ERR_INVALID_ARGUMENT, "num_scales must be 4.." + std::to_string(kDogMaxScales) +
+                                                     " (feature_detection.h:95 asserts >= 4)");
+    if (!(sigma0 > 0) || !std::isfinite(sigma0))
+        return fail(NDLGPU_ERR_BAD_SIGMA, "sigma0 must be positive and finite (feature_detection.h:96)");
+    if (!dogs) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "dogs is NULL");
+    const int ns = num_scales;
+    std::vector<const ndlgpu_view*> outs;
+    for (int i = 0; i < ns - 1; i++) outs.push_back(&dogs[i]);
+    if (levels)
+        for (int i = 0; i < ns; i++) outs.push_back(&levels[i]);
+    for (size_t i = 0; i < outs.size(); i++) {
+        const ndlgpu_view* o = outs[i];
+        if ((st = check_view(o, (int)i < ns - 1 ? "dogs[i]" : "levels[i]", true)) != NDLGPU_OK) return st;
+        if (o->dtype != NDLGPU_F32 && o->dtype != NDLGPU_F64)
+            return fail(NDLGPU_ERR_UNSUPPORTED_DTYPE, "levels and dogs must be F32 or F64 images");
+        if ((st = check_pair(src, o)) != NDLGPU_OK) return st;
+    }
+    if (view_count(src) == 0) return NDLGPU_OK;
+    for (size_t i = 0; i < outs.size(); i++)
+        for (size_t j = i + 1; j < outs.size(); j++) {
+            intptr_t a0, a1, b0, b1;
+            view_bytes(outs[i], &a0, &a1);
+            view_bytes(outs[j], &b0, &b1);
+            if (a0 < b1 && b0 < a1) return fail(NDLGPU_ERR_ALIASING, "two output images overlap");
+        }
+    // sigma_i = sigma0 * 2^(i / (num_scales - 3)), radius ceil(3 sigma_i)
+    std::vector<double> sig(ns);
+    int rmax = 0;
+    for (int i = 0; i < ns; i++) {
+        sig[i] = sigma0 * std::pow(2.0, (double)i / (ns - 3));
+        if (2 * kernel_size(sig[i]) + 1 > kMaxTaps) return fail(NDLGPU_ERR_TOO_MANY_TAPS, "sigma too large (more than 255 taps)");
+        rmax = std::max(rmax, kernel_size(sig[i]));
+    }
+    for (int a = 0; a < src->rank; a++)
+        if (rmax > src->extent[a])
+            return fail(NDLGPU_ERR_RADIUS_EXCEEDS_EXTENT, "the largest level's radius " + std::to_string(rmax) +
+                                                               " exceeds extent " + std::to_string(src->extent[a]) +
+                                                               " (Reflect maps one period, mathHelpers.h:24)");
+    const cudaStream_t s = (cudaStream_t)stream;
+    bool all_f32 = true;
+    for (const ndlgpu_view* o : outs) all_f32 = all_f32 && o->dtype == NDLGPU_F32;
+    if (src->rank == 2 && all_f32 && ns <= kDogMaxLevels && rmax <= kDogMaxRadius && float_exact_dtype(src->dtype)) {
+        // one pass over the source (dog.cu)
+        DogParams p{};
+        p.src = static_cast<const char*>(src->data);
+        p.sdt = src->dtype;
+        p.nx = (int)src->extent[0];
+        p.ny = (int)src->extent[1];
+        p.sx = src->stride[0];
+        p.sy = src->stride[1];
+        p.ns = ns;
+        p.R = rmax;
+        for (int i = 0; i < ns; i++) {
+            const std::vector<double> w = gaussian_taps(sig[i]);
+            p.r[i] = (int)w.size() / 2;
+            for (size_t k = 0; k < w.size(); k++) p.w[i][k] = (float)w[k];
+            if (levels) {
+                p.lv[i] = static_cast<float*>(levels[i].data);
+                p.lx[i] = levels[i].stride[0];
+                p.ly[i] = levels[i].stride[1];
+            }
+            if (i > 0) {
+                p.dg[i - 1] = static_cast<float*>(dogs[i - 1].data);
+                p.gx[i - 1] = dogs[i - 1].stride[0];
+                p.gy[i - 1] = dogs[i - 1].stride[1];
+            }
+        }
+        cudaError_t e = launch_dog2d(p, s);
+        return e == cudaSuccess ? NDLGPU_OK : cuda_fail(e, "dog launch");
+    }
+    // any rank and type: one gaussian_blur per level, then the differences in
+    // double.  Levels go to the caller's level images when they have the
+    // differences' precision, else to two stream-ordered scratch images.
+    bool any_f64 = false;
+    for (int i = 0; i < ns - 1; i++) any_f64 = any_f64 || dogs[i].dtype == NDLGPU_F64;
+    const int ldt = any_f64 ? NDLGPU_F64 : NDLGPU_F32;
+    const int64_t count = view_count(src);
+    Scratch sc;
+    const bool own = !levels || levels[0].dtype != ldt;
+    for (int i = 0; levels && i < ns && !own; i++)
+        if (levels[i].dtype != ldt) return fail(NDLGPU_ERR_UNSUPPORTED_DTYPE, "level images must share one dtype");
+    ndlgpu_view tmp[2];
+    if (own) {
+        const size_t one = align_up((size_t)count * dtype_size(ldt));
+        if ((st = get_scratch(2 * one, nullptr, 0, s, &sc)) != NDLGPU_OK) return st;
+        for (int b = 0; b < 2; b++) {
+            tmp[b] = ndlgpu_view{};
+            tmp[b].data = static_cast<char*>(sc.base) + b * one;
+            tmp[b].dtype = ldt;
+            tmp[b].rank = src->rank;
+            int64_t stv = 1;
+            for (int a = 0; a < src->rank; a++) {
+                tmp[b].extent[a] = src->extent[a];
+                tmp[b].stride[a] = stv;
+                stv *= src->extent[a];
+            }
+        }
+    }
+    const ndlgpu_view* prev = nullptr;
+    for (int i = 0; i < ns; i++) {
+        const ndlgpu_view* cur = own ? &tmp[i & 1] : &levels[i];
+        if ((st = blur_level(src, cur, sig[i], s)) != NDLGPU_OK) return st;
+        if (own && levels && (st = blur_level(src, &levels[i], sig[i], s)) != NDLGPU_OK) return st;
+        if (prev) {
+            const ndlgpu_view& d = dogs[i - 1];
+            SubParams sp{};
+            sp.a = static_cast<const char*>(cur->data);
+            sp.b = static_cast<const char*>(prev->data);
+            sp.dst = static_cast<char*>(d.data);
+            sp.adt = cur->dtype;
+            sp.bdt = prev->dtype;
+            sp.ddt = d.dtype;
+            sp.rank = src->rank;
+            sp.total = count;
+            for (int a = 0; a < src->rank; a++) {
+                sp.ext[a] = src->extent[a];
+                sp.as[a] = cur->stride[a];
+                sp.bs[a] = prev->stride[a];
+                sp.ds[a] = d.stride[a];
+            }
+            cudaError_t e = launch_sub(sp, s);
+            if (e != cudaSuccess) return cuda_fail(e, "dog difference launch");
+        }
+        prev = cur;
+    }
+    return NDLGPU_OK;
+}
+
 ndlgpu_status ndlgpu_convolve(const ndlgpu_view* src, const ndlgpu_view* dst, const ndlgpu_view* kernel, int border,
                               void* stream)
 {

@@ -259,6 +259,37 @@ struct GradParams {
 bool gradient_supported(const GradParams& p);
 cudaError_t launch_gradient(const GradParams& p, cudaStream_t s);
 
+// Difference-of-Gaussians scale space (dog.cu).
+constexpr int kDogMaxLevels = 16;      // fused kernel; the per-level path takes up to kDogMaxScales
+constexpr int kDogMaxScales = 64;
+constexpr int kDogMaxRadius = 48;
+struct DogParams {
+    const char* src;
+    int sdt;
+    int nx, ny;
+    int64_t sx, sy;                        // source strides, elements
+    int ns;                                // levels
+    int R;                                 // largest radius
+    int r[kDogMaxLevels];
+    float w[kDogMaxLevels][2 * kDogMaxRadius + 1];
+    float* lv[kDogMaxLevels];              // level outputs (NULL: not written)
+    int64_t lx[kDogMaxLevels], ly[kDogMaxLevels];
+    float* dg[kDogMaxLevels - 1];          // difference outputs
+    int64_t gx[kDogMaxLevels - 1], gy[kDogMaxLevels - 1];
+};
+size_t dog2d_smem_bytes(int R);
+cudaError_t launch_dog2d(const DogParams& p, cudaStream_t s);
+struct SubParams {                         // dst = a - b in double, any rank
+    const char* a;
+    const char* b;
+    char* dst;
+    int adt, bdt, ddt;
+    int rank;
+    int64_t total;
+    int64_t ext[kMaxRank], as[kMaxRank], bs[kMaxRank], ds[kMaxRank];
+};
+cudaError_t launch_sub(const SubParams& p, cudaStream_t s);
+
 // Batched form (batch.cu): one persistent launch over a table of instances.
 constexpr int kBatchMaxTaps = 37;
 struct BatchDesc {

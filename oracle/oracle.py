@@ -81,7 +81,8 @@ def _load_ref():
         if not have_reference():
             raise RuntimeError("reference shim not built (oracle/build_oracle.py needs the ndl source tree)")
         _ref = ctypes.CDLL(reference_path())
-        for name in ("ref_convolve", "ref_gaussian_blur", "ref_compose", "ref_view_probe", "ref_gradient"):
+        for name in ("ref_convolve", "ref_gaussian_blur", "ref_compose", "ref_view_probe", "ref_gradient",
+                     "ref_detect_keypoints"):
             getattr(_ref, name).restype = ctypes.c_int
     return _ref
 
@@ -277,6 +278,50 @@ def gaussian_blur(src, sigma, border=CLAMP, out_code=None, code=None):
     return compose(src, [(a, w) for a in range(ndim)], border, out_code, STORE_ROUND, code)
 
 
+def dog_sigmas(num_scales, sigma0):
+    """sigma_i = sigma0 * 2^(i / (num_scales - 3)), feature_detection.h:105-107."""
+    return [sigma0 * 2.0 ** (i / (num_scales - 3)) for i in range(num_scales)]
+
+
+def dog_scale_space(src, num_scales=5, sigma0=1.6, code=None):
+    """Levels and Difference-of-Gaussians of detect_keypoints
+    (processing/feature_detection.h:101-122), in double: level i is
+    gaussian_blur(src as double, sigma_i, Reflect) (no final cast: double
+    output), dog[i] = level[i+1] - level[i].  Returns (levels, dogs)."""
+    x = to_f64(src, code)
+    levels = []
+    for s in dog_sigmas(num_scales, sigma0):
+        w = gaussian_weights(s)
+        levels.append(compose_total(x, [(a, w) for a in range(x.ndim)], REFLECT))
+    return levels, [levels[i + 1] - levels[i] for i in range(num_scales - 1)]
+
+
+def dog_keypoints(dogs, sigmas, threshold):
+    """The extrema search of detect_keypoints (feature_detection.h:131-160):
+    on every interior layer, positions with |v| >= threshold that are a strict
+    max or min against the 3^D - 1 same-layer and 2 * 3^D adjacent-layer
+    neighbours, Clamp at the border.  Returns sorted (position (ndl axis
+    order), scale, response) tuples."""
+    import itertools
+    D = dogs[0].ndim
+    out = []
+    for layer in range(1, len(dogs) - 1):
+        v = dogs[layer]
+        pads = [np.pad(dogs[layer + d], 1, mode="edge") for d in (-1, 0, 1)]
+        ismax = np.abs(v) >= threshold
+        ismin = ismax.copy()
+        for d in (-1, 0, 1):
+            for off in itertools.product((0, 1, 2), repeat=D):
+                if d == 0 and all(o == 1 for o in off):
+                    continue
+                n = pads[d + 1][tuple(slice(o, o + v.shape[i]) for i, o in enumerate(off))]
+                ismax &= n < v
+                ismin &= n > v
+        for idx in np.argwhere(ismax | ismin):
+            out.append((tuple(int(i) for i in idx[::-1]), sigmas[layer], float(abs(v[tuple(idx)]))))
+    return sorted(out)
+
+
 def compose_adjoint(g, x, passes, border=CLAMP):
     """FP64 adjoint of the composition Y = P_n(...P_1(X)) for
     L = sum(g * Y): returns (dL/dX, [dL/dw_p for each pass])."""
@@ -327,6 +372,24 @@ def ref_gradient(src, border=REFLECT, out_dtype=None):
     if rc != 0:
         raise RuntimeError("ref_gradient failed (%d)" % rc)
     return out
+
+
+def ref_detect_keypoints(src, num_scales=5, sigma0=1.6, threshold=5.0, max_n=100000):
+    """Runs ndl::detect_keypoints() itself on src as a double image; returns
+    sorted (position (ndl axis order), scale, response) tuples."""
+    lib = _load_ref()
+    x = np.ascontiguousarray(src, dtype=np.float64)
+    D = x.ndim
+    pos = np.zeros(max_n * D, np.int32)
+    sc = np.zeros(max_n, np.float64)
+    rs = np.zeros(max_n, np.float64)
+    n = lib.ref_detect_keypoints(D, x.ctypes.data_as(_f64p), _i32arr(x.shape[::-1]), int(num_scales),
+                                 ctypes.c_double(sigma0), ctypes.c_double(threshold),
+                                 pos.ctypes.data_as(_i32p), sc.ctypes.data_as(_f64p), rs.ctypes.data_as(_f64p),
+                                 int(max_n))
+    if n < 0:
+        raise RuntimeError("more than %d keypoints" % max_n)
+    return sorted((tuple(int(v) for v in pos[k * D:(k + 1) * D]), float(sc[k]), float(rs[k])) for k in range(n))
 
 
 def ref_gaussian_blur(src, sigma, border=CLAMP, out_dtype=None, out=None):

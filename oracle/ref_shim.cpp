@@ -13,8 +13,11 @@
 // product Image::at() computes (image/core.h:557-558).  ref_view_probe() runs
 // the reference's real Image view builders (view/swap_axes/mirror,
 // image/core.h:647-757) so the host-side view arithmetic can be pinned to it.
+// ref_detect_keypoints() runs ndl::detect_keypoints() itself, whose keypoints
+// carry the Difference-of-Gaussians values (processing/feature_detection.h).
 #include <ndl/image.h>
 #include <ndl/processing/convolution.h>
+#include <ndl/processing/feature_detection.h>
 
 #include <array>
 #include <cstdint>
@@ -118,6 +121,29 @@ ndl::Image<double, DIM> axis_kernel(int axis, int K, const double* w, std::vecto
 }  // namespace
 
 extern "C" {
+
+// ndl::detect_keypoints(src, num_scales, sigma0, threshold) on a contiguous
+// double image (axis 0 fastest).  Writes up to max_n keypoints -- position
+// (dim ints each), scale and response -- and returns their count, or -1 when
+// there are more than max_n.
+int ref_detect_keypoints(int dim, double* src, const int* ext, int num_scales, double sigma0, double threshold,
+                         int* pos, double* scale, double* response, int max_n)
+{
+    return dispatch_dim(dim, [&](auto D) {
+        constexpr int DIM = decltype(D)::value;
+        std::array<int, DIM> e;
+        for (int i = 0; i < DIM; i++) e[i] = ext[i];
+        ndl::Image<double, DIM> img(src, e);
+        const auto kps = ndl::detect_keypoints(img, num_scales, sigma0, threshold);
+        if ((int)kps.size() > max_n) return -1;
+        for (size_t k = 0; k < kps.size(); k++) {
+            for (int i = 0; i < DIM; i++) pos[k * DIM + i] = kps[k].position[i];
+            scale[k] = kps[k].scale;
+            response[k] = kps[k].response;
+        }
+        return (int)kps.size();
+    });
+}
 
 // ndl::gradient(src, dst, border) (processing/convolution.h:359-388): dst of
 // extent {dim, ext...} with strides dstr[0..dim].
