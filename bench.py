@@ -483,6 +483,17 @@ def other_forms(args, hbm):
                                  "frac_of_measured_hbm": round(16.0 * vox / ms / 1e6 / hbm, 4)}
     del x, s, o
     out["dog_f32_4096^2_5scales"] = dog_form(g, it, hbm)
+    # downsample (convolution.h:241-305): a {3, 15360, 8640} uint8 colour
+    # image (channel axis 0, 398 MB) by 2; algorithmic bytes = source + result
+    x = torch.randint(0, 256, (8640, 15360, 3), generator=g, device="cuda", dtype=torch.uint8)
+    s = Image.from_tensor(x)
+    o = Image.empty([3, 7680, 4320], torch.uint8)
+    ms = time_call(lambda: n.downsample(s, 2, 0, dst=o), it)
+    nb = x.numel() * 1.25
+    out["downsample_u8_rgb_15360x8640_f2"] = {"ms": round(ms, 4), "gbs": round(nb / ms / 1e6, 1),
+                                              "frac_of_measured_hbm": round(nb / ms / 1e6 / hbm, 4),
+                                              "exact": "bit-exact block averages"}
+    del x, s, o
     # config 5: 4-D video 1024x1024x3x96, sigma (2.5, 2.5, -, 1.5), Reflect
     for name, dt in (("video_bf16", torch.bfloat16), ("video_f16", torch.float16), ("video_f32", torch.float32)):
         v = torch.rand((96, 3, 1024, 1024), generator=g, device="cuda", dtype=torch.float32)

@@ -147,6 +147,18 @@ NDLGPU_API ndlgpu_status ndlgpu_convolve_ex(const ndlgpu_view* src, const ndlgpu
  * The reference's default border is Reflect. */
 NDLGPU_API ndlgpu_status ndlgpu_gradient(const ndlgpu_view* src, const ndlgpu_view* dst, int border, void* stream);
 
+/* ndl::downsample(src, factor, channelAxis, border) -- processing/convolution.h:241-305.
+ * Every axis but channel_axis shrinks to (extent - 1) / factor + 1 (dst must
+ * have those extents; the reference returns a new image of them); each
+ * output is the average of its non-overlapping factor-wide source block (a
+ * short last block averages the samples that exist), summed in double in the
+ * reference's block order and then std::round-ed for integral dst types, so
+ * the results equal the reference's bit for bit when dst has src's type.
+ * factor > 1; rank >= 2; `border` is accepted and unused, as in the
+ * reference. */
+NDLGPU_API ndlgpu_status ndlgpu_downsample(const ndlgpu_view* src, const ndlgpu_view* dst, int factor,
+                                           int channel_axis, int border, void* stream);
+
 /* The Difference-of-Gaussians scale space of ndl::detect_keypoints
  * (processing/feature_detection.h:101-122): num_scales (4..64) levels,
  * level i = gaussian_blur(src as double, sigma_i, Reflect) with

@@ -90,6 +90,7 @@ SIGNATURES = {
     "ndlgpu_convolve_ex": (_I, [_PV, _PV, _PV, _I, _I, _VP]),
     "ndlgpu_gradient": (_I, [_PV, _PV, _I, _VP]),
     "ndlgpu_dog_scale_space": (_I, [_PV, _I, ctypes.c_double, _PV, _PV, _VP]),
+    "ndlgpu_downsample": (_I, [_PV, _PV, _I, _I, _I, _VP]),
     "ndlgpu_gaussian_blur": (_I, [_PV, _PV, ctypes.c_double, _I, _VP, _SZ, _VP]),
     "ndlgpu_gaussian_blur_workspace_size": (_I, [_PV, _PV, ctypes.c_double, _I, ctypes.POINTER(_SZ)]),
     "ndlgpu_gaussian_blur_axes": (_I, [_PV, _PV, ctypes.POINTER(ctypes.c_double), _I, _VP, _SZ, _VP]),

@@ -72,6 +72,21 @@ def gradient(src: Image, dst: Image = None, border=BorderMode.Reflect, stream=No
     return dst
 
 
+def downsample(src: Image, factor: int, channel_axis=0, border=BorderMode.Clamp, dst: Image = None, stream=None):
+    """ndl::downsample(src, factor, channelAxis, border)
+    (processing/convolution.h:241-305): every axis but channel_axis shrinks
+    by factor, each output the average of its non-overlapping block (rounded
+    for integral types).  Returns dst (made in src's type when None)."""
+    ext = [e if a == channel_axis else (e - 1) // factor + 1 for a, e in enumerate(src.extent())]
+    if dst is None:
+        dst = Image.empty(ext, src.dtype)
+    lib = abi.load()
+    sv, dv = src.abi_view(), dst.abi_view()
+    abi.check(lib.ndlgpu_downsample(ctypes.byref(sv), ctypes.byref(dv), int(factor), int(channel_axis), int(border),
+                                    _stream_ptr(stream)))
+    return dst
+
+
 def dog_scale_space(src: Image, num_scales=5, sigma0=1.6, dogs=None, levels=None, dtype=None, stream=None):
     """The Difference-of-Gaussians scale space of ndl::detect_keypoints
     (processing/feature_detection.h:101-122): level i is

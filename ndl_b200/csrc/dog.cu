@@ -8,16 +8,20 @@
 // level and difference from it.  A CTA owns 64 x 32 outputs.  It loads the
 // tile with the largest level's halo once (Reflect-mapped, converted to
 // float) into shared memory, then per level runs the X pass over the rows
-// that level's Y pass needs (one unit = 4 outputs from a rolling register
-// window; lanes of a warp take consecutive rows, conflict-free on the odd
-// pitch), then the Y pass (8 rows per thread, rolling window down a column),
-// keeps the level in registers and writes level - previous level.  The
+// that level's Y pass needs (one unit = 2 rows x 4 outputs as packed FP32
+// pairs; lanes of a warp take consecutive rows, conflict-free on the odd
+// pitch), then the Y pass (2 columns x 4 rows per thread, packed), keeps the
+// level in registers and writes level - previous level.  Both passes keep
+// their sample window in slots indexed by tap mod 4 (an unrolled-by-4 tap
+// loop), so no value is ever moved between registers.  The
 // source is read once instead of num_scales times, and no level goes through
 // HBM unless the caller asks for it.
 //
 // k_sub_nd: dst = a - b elementwise in double for any rank, dtype and
 // strides (the differences of the per-level path for other ranks and for
 // FP64 results).
+#include <type_traits>
+
 #include "dtype.cuh"
 
 namespace ndlgpu {
@@ -37,6 +41,30 @@ __device__ __forceinline__ int reflect_tile(int x, int n)
     return m < 0 ? 0 : (m >= n ? n - 1 : m);
 }
 
+template <class T> __device__ __forceinline__ float src_f(const T* p, int64_t i);
+template <> __device__ __forceinline__ float src_f<float>(const float* p, int64_t i) { return __ldg(p + i); }
+template <> __device__ __forceinline__ float src_f<uint8_t>(const uint8_t* p, int64_t i) { return (float)__ldg(p + i); }
+template <> __device__ __forceinline__ float src_f<__half>(const __half* p, int64_t i) { return __half2float(__ldg(p + i)); }
+template <> __device__ __forceinline__ float src_f<__nv_bfloat16>(const __nv_bfloat16* p, int64_t i)
+{
+    return __bfloat162float(__ldg(p + i));
+}
+
+// Stores of one output pair (columns ox, ox+1 of row oy).
+__device__ __forceinline__ void store_pair(float* base, int64_t sx, int64_t sy, int vec, int ox, int oy, int nx,
+                                           float2 v)
+{
+    float* q = base + (int64_t)ox * sx + (int64_t)oy * sy;
+    if (vec && ox + 1 < nx) {
+        *reinterpret_cast<float2*>(q) = v;
+    } else {
+        if (ox < nx) q[0] = v.x;
+        if (ox + 1 < nx) q[sx] = v.y;
+    }
+}
+
+// T: the source type (void: any exact-in-float type through load_as).
+template <class T>
 __global__ void __launch_bounds__(DNT, 2) k_dog2d(const __grid_constant__ DogParams p)
 {
     extern __shared__ __align__(16) float sm[];
@@ -47,67 +75,86 @@ __global__ void __launch_bounds__(DNT, 2) k_dog2d(const __grid_constant__ DogPar
     float* s_src = sm;
     float* s_x = sm + ((SH * SP + 3) & ~3);
     const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
     const int x0 = blockIdx.x * DTX;
     const int y0 = blockIdx.y * DTY;
 
-    for (int i = tid; i < SH * SW; i += DNT) {
-        const int r = i / SW, c = i - r * SW;
-        const int gy = reflect_tile(y0 - R + r, p.ny);
-        const int gx = reflect_tile(x0 - R + c, p.nx);
-        s_src[r * SP + c] = load_as<float>(p.src, p.sdt, (int64_t)gx * p.sx + (int64_t)gy * p.sy);
+    // the tile with the largest halo, Reflect-mapped, as float
+    for (int r = warp; r < SH; r += DNT / 32) {
+        const int64_t rowoff = (int64_t)reflect_tile(y0 - R + r, p.ny) * p.sy;
+        for (int c = lane; c < SW; c += 32) {
+            const int64_t i = rowoff + (int64_t)reflect_tile(x0 - R + c, p.nx) * p.sx;
+            float v;
+            if constexpr (std::is_void<T>::value) v = load_as<float>(p.src, p.sdt, i);
+            else v = src_f<T>(reinterpret_cast<const T*>(p.src), i);
+            s_src[r * SP + c] = v;
+        }
     }
     __syncthreads();
 
-    const int tx = tid & (DTX - 1);
-    const int tg = tid / DTX;
-    const int ox = x0 + tx;
-    float prev[8];
+    // Y-pass outputs of this thread: columns cx, cx+1 of rows ry .. ry+3
+    const int cx = 2 * lane;
+    const int ry = 4 * warp;
+    const int ox = x0 + cx;
+    float2 prev[4];
 #pragma unroll
-    for (int j = 0; j < 8; j++) prev[j] = 0.f;
+    for (int j = 0; j < 4; j++) prev[j] = make_float2(0.f, 0.f);
 
     for (int s = 0; s < p.ns; s++) {
         const int r = p.r[s];
         const int K = 2 * r + 1;
-        const int rows = DTY + 2 * r;
-        const float* w = p.w[s];
-        // X pass: unit u = (row u % rows, columns 4g .. 4g+3 with g = u / rows)
-        for (int u = tid; u < rows * (DTX / 4); u += DNT) {
-            const int g = u / rows, row = u - g * rows;
-            const float* sp = s_src + (row + R - r) * SP + 4 * g + (R - r);
-            float v0 = sp[0], v1 = sp[1], v2 = sp[2];
-            float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
-#pragma unroll 4
-            for (int k = 0; k < K; k++) {
-                const float v3 = sp[k + 3];
-                const float wk = w[k];
-                a0 = fmaf(v0, wk, a0);
-                a1 = fmaf(v1, wk, a1);
-                a2 = fmaf(v2, wk, a2);
-                a3 = fmaf(v3, wk, a3);
-                v0 = v1;
-                v1 = v2;
-                v2 = v3;
+        const int H = DTY / 2 + r;     // X-pass rows come in pairs (i, i + H)
+        const float2* w2 = p.w2[s];
+        // X pass: unit u = rows (i, i+H) x columns 4g .. 4g+3, packed as
+        // (row i, row i+H) pairs; lanes take consecutive i (odd pitch: no
+        // bank conflicts).  Window slot m holds column offset k+m (mod 4), so
+        // the window never moves.
+        for (int u = tid; u < H * (DTX / 4); u += DNT) {
+            const int g = u / H, i = u - g * H;
+            const float* s0 = s_src + (i + R - r) * SP + 4 * g + (R - r);
+            const float* s1 = s0 + H * SP;
+            float2 wv[4];
+            wv[0] = make_float2(s0[0], s1[0]);
+            wv[1] = make_float2(s0[1], s1[1]);
+            wv[2] = make_float2(s0[2], s1[2]);
+            wv[3] = make_float2(0.f, 0.f);
+            float2 a[4] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f),
+                           make_float2(0.f, 0.f)};
+            for (int k = 0; k < K; k += 4) {
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    if (k + q < K) {
+                        wv[(q + 3) & 3] = make_float2(s0[k + q + 3], s1[k + q + 3]);
+                        const float2 wk = w2[k + q];
+#pragma unroll
+                        for (int m = 0; m < 4; m++) a[m] = __ffma2_rn(wv[(q + m) & 3], wk, a[m]);
+                    }
+                }
             }
-            *reinterpret_cast<float4*>(s_x + row * XP + 4 * g) = make_float4(a0, a1, a2, a3);
+            *reinterpret_cast<float4*>(s_x + i * XP + 4 * g) = make_float4(a[0].x, a[1].x, a[2].x, a[3].x);
+            *reinterpret_cast<float4*>(s_x + (i + H) * XP + 4 * g) = make_float4(a[0].y, a[1].y, a[2].y, a[3].y);
         }
         __syncthreads();
-        // Y pass: rows 8tg .. 8tg+7 of column tx
-        float cur[8];
+        // Y pass: (column cx, column cx+1) pairs down rows ry .. ry+3 with
+        // the same slot rotation
+        float2 cur[4] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
         {
-            const float* xp = s_x + 8 * tg * XP + tx;
-            float v[8];
+            const float* xp = s_x + ry * XP + cx;
+            float2 v[4];
+            v[0] = *reinterpret_cast<const float2*>(xp);
+            v[1] = *reinterpret_cast<const float2*>(xp + XP);
+            v[2] = *reinterpret_cast<const float2*>(xp + 2 * XP);
+            v[3] = make_float2(0.f, 0.f);
+            for (int k = 0; k < K; k += 4) {
 #pragma unroll
-            for (int j = 0; j < 7; j++) v[j] = xp[j * XP];
+                for (int q = 0; q < 4; q++) {
+                    if (k + q < K) {
+                        v[(q + 3) & 3] = *reinterpret_cast<const float2*>(xp + (k + q + 3) * XP);
+                        const float2 wk = w2[k + q];
 #pragma unroll
-            for (int j = 0; j < 8; j++) cur[j] = 0.f;
-#pragma unroll 2
-            for (int k = 0; k < K; k++) {
-                v[7] = xp[(k + 7) * XP];
-                const float wk = w[k];
-#pragma unroll
-                for (int j = 0; j < 8; j++) cur[j] = fmaf(v[j], wk, cur[j]);
-#pragma unroll
-                for (int j = 0; j < 7; j++) v[j] = v[j + 1];
+                        for (int j = 0; j < 4; j++) cur[j] = __ffma2_rn(v[(q + j) & 3], wk, cur[j]);
+                    }
+                }
             }
         }
         __syncthreads();    // the next level's X pass reuses s_x
@@ -115,15 +162,17 @@ __global__ void __launch_bounds__(DNT, 2) k_dog2d(const __grid_constant__ DogPar
             float* lv = p.lv[s];
             float* dg = s > 0 ? p.dg[s - 1] : nullptr;
 #pragma unroll
-            for (int j = 0; j < 8; j++) {
-                const int oy = y0 + 8 * tg + j;
+            for (int j = 0; j < 4; j++) {
+                const int oy = y0 + ry + j;
                 if (oy >= p.ny) break;
-                if (lv) lv[(int64_t)ox * p.lx[s] + (int64_t)oy * p.ly[s]] = cur[j];
-                if (dg) dg[(int64_t)ox * p.gx[s - 1] + (int64_t)oy * p.gy[s - 1]] = cur[j] - prev[j];
+                if (lv) store_pair(lv, p.lx[s], p.ly[s], p.lvec[s], ox, oy, p.nx, cur[j]);
+                if (dg)
+                    store_pair(dg, p.gx[s - 1], p.gy[s - 1], p.gvec[s - 1], ox, oy, p.nx,
+                               make_float2(cur[j].x - prev[j].x, cur[j].y - prev[j].y));
             }
         }
 #pragma unroll
-        for (int j = 0; j < 8; j++) prev[j] = cur[j];
+        for (int j = 0; j < 4; j++) prev[j] = cur[j];
     }
 }
 
@@ -156,13 +205,22 @@ cudaError_t launch_dog2d(const DogParams& p, cudaStream_t s)
     const size_t smem = dog2d_smem_bytes(p.R);
     static size_t configured = 0;
     if (smem > configured) {
-        cudaError_t e = cudaFuncSetAttribute(k_dog2d, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = cudaSuccess;
+        for (const void* k : {(const void*)k_dog2d<float>, (const void*)k_dog2d<uint8_t>, (const void*)k_dog2d<__half>,
+                              (const void*)k_dog2d<__nv_bfloat16>, (const void*)k_dog2d<void>})
+            if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         configured = smem;
     }
     const dim3 grid((unsigned)((p.nx + DTX - 1) / DTX), (unsigned)((p.ny + DTY - 1) / DTY));
     if (grid.y > 65535) return cudaErrorInvalidConfiguration;
-    k_dog2d<<<grid, DNT, smem, s>>>(p);
+    switch (p.sdt) {
+    case NDLGPU_F32: k_dog2d<float><<<grid, DNT, smem, s>>>(p); break;
+    case NDLGPU_U8: k_dog2d<uint8_t><<<grid, DNT, smem, s>>>(p); break;
+    case NDLGPU_F16: k_dog2d<__half><<<grid, DNT, smem, s>>>(p); break;
+    case NDLGPU_BF16: k_dog2d<__nv_bfloat16><<<grid, DNT, smem, s>>>(p); break;
+    default: k_dog2d<void><<<grid, DNT, smem, s>>>(p); break;
+    }
     count_launch();
     return cudaGetLastError();
 }

@@ -83,6 +83,22 @@ static void view_bytes(const ndlgpu_view* v, intptr_t* lo, intptr_t* hi)
     *hi = (intptr_t)v->data + (intptr_t)mx * es + es;
 }
 
+// dst must not write one address twice: with axes sorted by |stride|, each
+// axis must step over everything the faster axes cover.
+static ndlgpu_status check_no_self_overlap(const ndlgpu_view* dst)
+{
+    std::vector<std::pair<int64_t, int64_t>> ax;
+    for (int i = 0; i < dst->rank; i++)
+        if (dst->extent[i] > 1) ax.push_back({dst->stride[i] < 0 ? -dst->stride[i] : dst->stride[i], dst->extent[i]});
+    std::sort(ax.begin(), ax.end());
+    int64_t covered = 1;
+    for (auto& a : ax) {
+        if (a.first < covered) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "dst view overlaps itself (a stride is smaller than the span of the faster axes)");
+        covered = a.first * a.second;
+    }
+    return NDLGPU_OK;
+}
+
 static ndlgpu_status check_pair(const ndlgpu_view* src, const ndlgpu_view* dst)
 {
     if (src->rank != dst->rank) return fail(NDLGPU_ERR_EXTENT_MISMATCH, "src and dst ranks differ");
@@ -94,18 +110,7 @@ static ndlgpu_status check_pair(const ndlgpu_view* src, const ndlgpu_view* dst)
     view_bytes(src, &a0, &a1);
     view_bytes(dst, &b0, &b1);
     if (a0 < b1 && b0 < a1) return fail(NDLGPU_ERR_ALIASING, "src and dst memory overlap (in-place convolution is not supported)");
-    // dst must not write one address twice: with axes sorted by |stride|,
-    // each axis must step over everything the faster axes cover.
-    std::vector<std::pair<int64_t, int64_t>> ax;
-    for (int i = 0; i < dst->rank; i++)
-        if (dst->extent[i] > 1) ax.push_back({dst->stride[i] < 0 ? -dst->stride[i] : dst->stride[i], dst->extent[i]});
-    std::sort(ax.begin(), ax.end());
-    int64_t covered = 1;
-    for (auto& a : ax) {
-        if (a.first < covered) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "dst view overlaps itself (a stride is smaller than the span of the faster axes)");
-        covered = a.first * a.second;
-    }
-    return NDLGPU_OK;
+    return check_no_self_overlap(dst);
 }
 
 // ---------------------------------------------------------------------------
@@ -1807,16 +1812,22 @@ ndlgpu_status ndlgpu_dog_scale_space(const ndlgpu_view* src, int num_scales, dou
         for (int i = 0; i < ns; i++) {
             const std::vector<double> w = gaussian_taps(sig[i]);
             p.r[i] = (int)w.size() / 2;
-            for (size_t k = 0; k < w.size(); k++) p.w[i][k] = (float)w[k];
+            for (size_t k = 0; k < w.size(); k++) p.w2[i][k] = make_float2((float)w[k], (float)w[k]);
+            // pair stores need x stride 1 and 8-byte aligned pairs on every row
+            auto pairs_ok = [](const ndlgpu_view& v) {
+                return v.stride[0] == 1 && reinterpret_cast<uintptr_t>(v.data) % 8 == 0 && v.stride[1] % 2 == 0;
+            };
             if (levels) {
                 p.lv[i] = static_cast<float*>(levels[i].data);
                 p.lx[i] = levels[i].stride[0];
                 p.ly[i] = levels[i].stride[1];
+                p.lvec[i] = pairs_ok(levels[i]);
             }
             if (i > 0) {
                 p.dg[i - 1] = static_cast<float*>(dogs[i - 1].data);
                 p.gx[i - 1] = dogs[i - 1].stride[0];
                 p.gy[i - 1] = dogs[i - 1].stride[1];
+                p.gvec[i - 1] = pairs_ok(dogs[i - 1]);
             }
         }
         cudaError_t e = launch_dog2d(p, s);
@@ -1878,6 +1889,50 @@ ndlgpu_status ndlgpu_dog_scale_space(const ndlgpu_view* src, int num_scales, dou
         prev = cur;
     }
     return NDLGPU_OK;
+}
+
+ndlgpu_status ndlgpu_downsample(const ndlgpu_view* src, const ndlgpu_view* dst, int factor, int channel_axis,
+                                int border, void* stream)
+{
+    // ndl::downsample (processing/convolution.h:241-305); `border` is accepted
+    // and unused, as in the reference (:262)
+    (void)border;
+    t_last_error.clear();
+    ndlgpu_status st;
+    if ((st = check_view(src, "src", true)) != NDLGPU_OK) return st;
+    if ((st = check_view(dst, "dst", true)) != NDLGPU_OK) return st;
+    if (factor < 2) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "factor must be > 1 (convolution.h:265)");
+    if (src->rank < 2) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "downsample needs a channel axis and at least one other");
+    if (channel_axis < 0 || channel_axis >= src->rank) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "channel_axis out of range");
+    if (dst->rank != src->rank) return fail(NDLGPU_ERR_EXTENT_MISMATCH, "src and dst ranks differ");
+    DownParams p{};
+    p.rank = src->rank;
+    p.channel = channel_axis;
+    p.factor = factor;
+    p.total = 1;
+    for (int a = 0; a < src->rank; a++) {
+        const int64_t oe = (a == channel_axis || src->extent[a] == 0) ? src->extent[a] : (src->extent[a] - 1) / factor + 1;
+        if (dst->extent[a] != oe)
+            return fail(NDLGPU_ERR_EXTENT_MISMATCH, "dst extent on axis " + std::to_string(a) + " must be " +
+                                                        std::to_string(oe) + " ((extent - 1) / factor + 1, convolution.h:268-269)");
+        p.ext[a] = (int)src->extent[a];
+        p.oext[a] = (int)oe;
+        p.sstr[a] = src->stride[a];
+        p.dstr[a] = dst->stride[a];
+        p.total *= oe;
+    }
+    if (p.total == 0) return NDLGPU_OK;
+    intptr_t a0, a1, b0, b1;
+    view_bytes(src, &a0, &a1);
+    view_bytes(dst, &b0, &b1);
+    if (a0 < b1 && b0 < a1) return fail(NDLGPU_ERR_ALIASING, "src and dst memory overlap");
+    if ((st = check_no_self_overlap(dst)) != NDLGPU_OK) return st;
+    p.src = static_cast<const char*>(src->data);
+    p.dst = static_cast<char*>(dst->data);
+    p.sdt = src->dtype;
+    p.ddt = dst->dtype;
+    cudaError_t e = launch_downsample(p, (cudaStream_t)stream);
+    return e == cudaSuccess ? NDLGPU_OK : cuda_fail(e, "downsample launch");
 }
 
 ndlgpu_status ndlgpu_convolve(const ndlgpu_view* src, const ndlgpu_view* dst, const ndlgpu_view* kernel, int border,

@@ -271,11 +271,13 @@ struct DogParams {
     int ns;                                // levels
     int R;                                 // largest radius
     int r[kDogMaxLevels];
-    float w[kDogMaxLevels][2 * kDogMaxRadius + 1];
+    float2 w2[kDogMaxLevels][2 * kDogMaxRadius + 1];   // (w, w) pairs of each level's taps
     float* lv[kDogMaxLevels];              // level outputs (NULL: not written)
     int64_t lx[kDogMaxLevels], ly[kDogMaxLevels];
+    int lvec[kDogMaxLevels];               // x stride 1, 8-byte aligned rows: pair stores
     float* dg[kDogMaxLevels - 1];          // difference outputs
     int64_t gx[kDogMaxLevels - 1], gy[kDogMaxLevels - 1];
+    int gvec[kDogMaxLevels - 1];
 };
 size_t dog2d_smem_bytes(int R);
 cudaError_t launch_dog2d(const DogParams& p, cudaStream_t s);
@@ -289,6 +291,21 @@ struct SubParams {                         // dst = a - b in double, any rank
     int64_t ext[kMaxRank], as[kMaxRank], bs[kMaxRank], ds[kMaxRank];
 };
 cudaError_t launch_sub(const SubParams& p, cudaStream_t s);
+
+// downsample (downsample.cu): block averages, every axis but the channel axis.
+struct DownParams {
+    const char* src;
+    char* dst;
+    int sdt, ddt;
+    int rank;
+    int channel;
+    int factor;
+    int ext[kMaxRank];                     // source extents
+    int oext[kMaxRank];                    // output extents
+    int64_t sstr[kMaxRank], dstr[kMaxRank];
+    int64_t total;                         // outputs
+};
+cudaError_t launch_downsample(const DownParams& p, cudaStream_t s);
 
 // Batched form (batch.cu): one persistent launch over a table of instances.
 constexpr int kBatchMaxTaps = 37;

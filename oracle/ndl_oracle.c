@@ -300,3 +300,53 @@ int ora_cast(const double* v, int64_t n, int dtype, int mode, void* out)
     }
     return 0;
 }
+
+/*
+ * downsample(src, factor, channelAxis) -- processing/convolution.h:241-305.
+ * Output extent: ext[a] on the channel axis, (ext[a] - 1) / factor + 1 on
+ * every other.  Each output is the double sum of its block -- source indices
+ * [o*factor, min(o*factor + factor, ext)) per non-channel axis -- walked as
+ * the reference's odometer walks it (the lowest non-channel axis fastest,
+ * :283-292), divided by the block's element count (:294).  The final cast
+ * (std::round for integral T) is ora_cast's.  out is contiguous, axis 0
+ * fastest.
+ */
+int ora_downsample(int dim, const double* src, const int64_t* ext, const int64_t* sstr, int factor, int channel,
+                   double* out)
+{
+    if (dim < 2 || dim > 16 || factor < 2 || channel < 0 || channel >= dim) return -1;
+    int64_t oext[16], oc[16], lo[16], hi[16], c[16];
+    for (int a = 0; a < dim; a++) {
+        oext[a] = (a == channel) ? ext[a] : (ext[a] - 1) / factor + 1;
+        oc[a] = 0;
+    }
+    const int64_t n = ora_count(dim, oext);
+    for (int64_t i = 0; i < n; i++) {
+        int64_t count = 1;
+        for (int a = 0; a < dim; a++) {
+            if (a == channel) {
+                lo[a] = oc[a];
+                hi[a] = oc[a] + 1;
+            } else {
+                lo[a] = oc[a] * factor;
+                hi[a] = lo[a] + factor < ext[a] ? lo[a] + factor : ext[a];
+                count *= hi[a] - lo[a];
+            }
+            c[a] = lo[a];
+        }
+        double sum = 0;
+        for (int64_t k = 0; k < count; k++) {
+            int64_t off = 0;
+            for (int a = 0; a < dim; a++) off += c[a] * sstr[a];
+            sum += src[off];
+            for (int a = 0; a < dim; a++) {
+                if (a == channel) continue;
+                if (++c[a] < hi[a]) break;
+                c[a] = lo[a];
+            }
+        }
+        out[i] = sum / (double)count;
+        ora_next(dim, oext, oc);
+    }
+    return 0;
+}

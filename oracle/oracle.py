@@ -55,7 +55,7 @@ def _load():
         if not os.path.exists(path):
             raise RuntimeError("oracle not built: run oracle/build_oracle.py")
         _lib = ctypes.CDLL(path)
-        for name in ("ora_convolve", "ora_axis_pass", "ora_axis_pass_adjoint", "ora_axis_tap_grad"):
+        for name in ("ora_convolve", "ora_axis_pass", "ora_axis_pass_adjoint", "ora_axis_tap_grad", "ora_downsample"):
             getattr(_lib, name).restype = ctypes.c_int
         _lib.ora_gaussian_weights.restype = ctypes.c_int
         _lib.ora_gaussian_weights.argtypes = [ctypes.c_double, _f64p]
@@ -82,7 +82,7 @@ def _load_ref():
             raise RuntimeError("reference shim not built (oracle/build_oracle.py needs the ndl source tree)")
         _ref = ctypes.CDLL(reference_path())
         for name in ("ref_convolve", "ref_gaussian_blur", "ref_compose", "ref_view_probe", "ref_gradient",
-                     "ref_detect_keypoints"):
+                     "ref_detect_keypoints", "ref_downsample", "ref_per_channel_blur"):
             getattr(_ref, name).restype = ctypes.c_int
     return _ref
 
@@ -278,6 +278,29 @@ def gaussian_blur(src, sigma, border=CLAMP, out_code=None, code=None):
     return compose(src, [(a, w) for a in range(ndim)], border, out_code, STORE_ROUND, code)
 
 
+def downsample_extent(shape, factor, channel_axis=0):
+    """numpy shape of downsample()'s result (channel_axis is an ndl axis)."""
+    D = len(shape)
+    ext = list(shape[::-1])
+    out = [e if a == channel_axis else (e - 1) // factor + 1 for a, e in enumerate(ext)]
+    return tuple(out[::-1])
+
+
+def downsample(src, factor, channel_axis=0, code=None, out_code=None):
+    """downsample(src, factor, channelAxis), processing/convolution.h:241-305:
+    block averages in double, then std::round for integral types (the result
+    type is src's unless out_code is given)."""
+    x = to_f64(src, code)
+    ext, st = _ndl_geom(x)
+    shape = downsample_extent(x.shape, factor, channel_axis)
+    out = np.zeros(shape, np.float64)
+    rc = _load().ora_downsample(x.ndim, x.ctypes.data_as(_f64p), _arr64(ext), _arr64(st), int(factor),
+                                int(channel_axis), out.ctypes.data_as(_f64p))
+    if rc != 0:
+        raise RuntimeError("ora_downsample failed")
+    return cast(out, dtype_code(src, code) if out_code is None else out_code, STORE_ROUND)
+
+
 def dog_sigmas(num_scales, sigma0):
     """sigma_i = sigma0 * 2^(i / (num_scales - 3)), feature_detection.h:105-107."""
     return [sigma0 * 2.0 ** (i / (num_scales - 3)) for i in range(num_scales)]
@@ -390,6 +413,43 @@ def ref_detect_keypoints(src, num_scales=5, sigma0=1.6, threshold=5.0, max_n=100
     if n < 0:
         raise RuntimeError("more than %d keypoints" % max_n)
     return sorted((tuple(int(v) for v in pos[k * D:(k + 1) * D]), float(sc[k]), float(rs[k])) for k in range(n))
+
+
+def per_channel_blur(src, sigma, channel_axis, border=CLAMP, code=None):
+    """per_channel(src, dst, channelAxis, gaussian_blur(., ., sigma, border))
+    (image/kernels.h:78-87): gaussian_blur's structure over every axis but
+    the channel axis (one remaining axis: a plain truncating convolve(),
+    convolution.h:141-146)."""
+    w = gaussian_weights(sigma)
+    D = np.asarray(src).ndim
+    passes = [(a, w) for a in range(D) if a != channel_axis]
+    return compose(src, passes, border, dtype_code(src, code), STORE_ROUND, code)
+
+
+def ref_per_channel_blur(src, sigma, channel_axis, border=CLAMP):
+    """Runs ndl::per_channel() with ndl::gaussian_blur() itself."""
+    lib = _load_ref()
+    x = np.ascontiguousarray(src)
+    out = np.zeros_like(x)
+    rc = lib.ref_per_channel_blur(x.ndim, dtype_code(x), ctypes.c_void_p(x.ctypes.data), _i32arr(x.shape[::-1]),
+                                  int(channel_axis), ctypes.c_double(sigma), int(border),
+                                  ctypes.c_void_p(out.ctypes.data))
+    if rc != 0:
+        raise RuntimeError("ref_per_channel_blur failed (%d)" % rc)
+    return out
+
+
+def ref_downsample(src, factor, channel_axis=0):
+    """Runs ndl::downsample() itself on a contiguous copy of src; returns its
+    result (src's dtype)."""
+    lib = _load_ref()
+    x = np.ascontiguousarray(src)
+    out = np.zeros(downsample_extent(x.shape, factor, channel_axis), x.dtype)
+    rc = lib.ref_downsample(x.ndim, dtype_code(x), ctypes.c_void_p(x.ctypes.data), _i32arr(x.shape[::-1]),
+                            int(factor), int(channel_axis), ctypes.c_void_p(out.ctypes.data))
+    if rc != 0:
+        raise RuntimeError("ref_downsample failed (%d)" % rc)
+    return out
 
 
 def ref_gaussian_blur(src, sigma, border=CLAMP, out_dtype=None, out=None):

@@ -122,6 +122,56 @@ ndl::Image<double, DIM> axis_kernel(int axis, int K, const double* w, std::vecto
 
 extern "C" {
 
+// ndl::per_channel(src, dst, channelAxis, fn) (image/kernels.h:78-87) with fn
+// = gaussian_blur(s, d, sigma, border) on every channel slice, on contiguous
+// images (axis 0 fastest) of one type.
+int ref_per_channel_blur(int dim, int tsrc, void* src, const int* ext, int channel_axis, double sigma, int border,
+                         void* dst)
+{
+    return dispatch_dim(dim, [&](auto D) {
+        constexpr int DIM = decltype(D)::value;
+        if constexpr (DIM < 2) {
+            return -4;
+        } else {
+            return dispatch_type(tsrc, [&](auto s) {
+                using S = decltype(s);
+                std::array<int, DIM> e;
+                for (int i = 0; i < DIM; i++) e[i] = ext[i];
+                ndl::Image<S, DIM> in(static_cast<S*>(src), e);
+                ndl::Image<S, DIM> out(static_cast<S*>(dst), e);
+                const ndl::BorderMode b = to_border(border);
+                ndl::per_channel(in, out, channel_axis, [&](auto si, auto di) { ndl::gaussian_blur(si, di, sigma, b); });
+                return 0;
+            });
+        }
+    });
+}
+
+// ndl::downsample(src, factor, channelAxis) (processing/convolution.h:241-305)
+// on a contiguous image (axis 0 fastest); its result, of src's type, is
+// copied to dst (contiguous).
+int ref_downsample(int dim, int tsrc, void* src, const int* ext, int factor, int channel_axis, void* dst)
+{
+    return dispatch_dim(dim, [&](auto D) {
+        constexpr int DIM = decltype(D)::value;
+        if constexpr (DIM < 2) {
+            return -4;
+        } else {
+            return dispatch_type(tsrc, [&](auto s) {
+                using S = decltype(s);
+                std::array<int, DIM> e;
+                for (int i = 0; i < DIM; i++) e[i] = ext[i];
+                ndl::Image<S, DIM> img(static_cast<S*>(src), e);
+                auto out = ndl::downsample(img, factor, channel_axis);
+                S* o = static_cast<S*>(dst);
+                size_t k = 0;
+                for (const auto& c : out.coordinates()) o[k++] = out.at(c);
+                return 0;
+            });
+        }
+    });
+}
+
 // ndl::detect_keypoints(src, num_scales, sigma0, threshold) on a contiguous
 // double image (axis 0 fastest).  Writes up to max_n keypoints -- position
 // (dim ints each), scale and response -- and returns their count, or -1 when

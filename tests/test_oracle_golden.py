@@ -228,3 +228,40 @@ def test_dog_oracle_matches_detect_keypoints(shape, ns, s0):
         ours = O.dog_keypoints(dogs, O.dog_sigmas(ns, s0), thr)
         assert len(ref) >= 5
         assert ref == ours
+
+
+def test_downsample_known_answers():
+    """image_convolution_tests.cpp:70-92: a constant {3, 40, 30} uint8 colour
+    image (channel axis 0) downsamples by 2 to {3, 20, 15}, still constant."""
+    x = np.full((30, 40, 3), 77, np.uint8)           # ndl extent {3, 40, 30}
+    out = O.downsample(x, 2, 0)
+    assert out.shape == (15, 20, 3) and (out == 77).all()
+    # a short last block averages only the samples that exist (:273-277)
+    y = np.arange(10, dtype=np.float64).reshape(2, 5)  # ndl {5, 2}; channel axis 1
+    assert (O.downsample(y, 2, 1) == np.array([[0.5, 2.5, 4.0], [5.5, 7.5, 9.0]])).all()
+
+
+@pytest.mark.skipif(not O.have_reference(), reason="compiled reference not present")
+@pytest.mark.parametrize("shape,factor,ch", [((30, 40, 3), 2, 0), ((31, 17, 3), 3, 0), ((9, 10, 11), 4, 1),
+                                             ((5, 7, 9, 2), 2, 3), ((33, 21), 5, 1), ((6, 50), 7, 0)])
+def test_downsample_oracle_matches_compiled_reference(shape, factor, ch):
+    rng = np.random.default_rng(factor + ch)
+    for dt in (np.uint8, np.int16, np.int32, np.float32, np.float64):
+        if np.issubdtype(dt, np.integer):
+            x = (rng.random(shape) * 250 - (120 if dt != np.uint8 else 0)).astype(dt)
+        else:
+            x = rng.standard_normal(shape).astype(dt)
+        assert (O.ref_downsample(x, factor, ch) == O.downsample(x, factor, ch)).all(), dt
+
+
+@pytest.mark.skipif(not O.have_reference(), reason="compiled reference not present")
+@pytest.mark.parametrize("shape,ch", [((30, 40, 3), 0), ((3, 17, 29), 2), ((40, 3), 0), ((12, 13, 14, 2), 0)])
+def test_per_channel_blur_oracle_matches_compiled_reference(shape, ch):
+    """per_channel(src, dst, channelAxis, gaussian_blur) (image/kernels.h:78-87)
+    is gaussian_blur's structure over the other axes -- with a single other
+    axis, the plain truncating convolve() of gaussian_blur's 1-D branch."""
+    rng = np.random.default_rng(len(shape) + ch)
+    for dt in (np.uint8, np.int16, np.float32):
+        x = (rng.random(shape) * 200).astype(dt)
+        for b in (0, 1, 2):
+            assert (O.ref_per_channel_blur(x, 1.3, ch, b) == O.per_channel_blur(x, 1.3, ch, b)).all(), (dt, b)
