@@ -1922,6 +1922,11 @@ ndlgpu_status ndlgpu_downsample(const ndlgpu_view* src, const ndlgpu_view* dst, 
         p.total *= oe;
     }
     if (p.total == 0) return NDLGPU_OK;
+    if (p.total > 0xffffffffLL) return fail(NDLGPU_ERR_INDEX_OVERFLOW, "downsample writes at most 2^32-1 outputs per call");
+    for (int a = 0; a < src->rank; a++) {
+        p.odiv[a].init((uint32_t)p.oext[a]);
+        if (a != channel_axis) p.sub[p.nsub++] = a;
+    }
     intptr_t a0, a1, b0, b1;
     view_bytes(src, &a0, &a1);
     view_bytes(dst, &b0, &b1);

@@ -303,7 +303,10 @@ struct DownParams {
     int ext[kMaxRank];                     // source extents
     int oext[kMaxRank];                    // output extents
     int64_t sstr[kMaxRank], dstr[kMaxRank];
-    int64_t total;                         // outputs
+    int64_t total;                         // outputs (< 2^32)
+    FastDiv odiv[kMaxRank];                // divisions by oext
+    int nsub;                              // non-channel axes, ascending
+    int sub[kMaxRank];
 };
 cudaError_t launch_downsample(const DownParams& p, cudaStream_t s);
 
