@@ -494,6 +494,19 @@ def other_forms(args, hbm):
                                               "frac_of_measured_hbm": round(nb / ms / 1e6 / hbm, 4),
                                               "exact": "bit-exact block averages"}
     del x, s, o
+    # box_blur (summed_area_table.h:300-339): 4096^2 f32, radius 8, Clamp,
+    # the reference's double summed-area table (bit-exact)
+    x = torch.rand((4096, 4096), generator=g, device="cuda")
+    s = Image.from_tensor(x)
+    o = Image.empty(s.extent(), torch.float32)
+    ws = torch.empty(n.box_blur_workspace_size(s, o, 8), dtype=torch.uint8, device="cuda")
+    ms = time_call(lambda: n.box_blur(s, o, 8, BorderMode.Clamp, workspace=ws), it)
+    out["box_blur_f32_4096^2_r8"] = {"ms": round(ms, 4), "mpix_s": round(x.numel() / ms / 1e3, 1),
+                                     "gbs": round(8.0 * x.numel() / ms / 1e6, 1),
+                                     "frac_of_measured_hbm": round(8.0 * x.numel() / ms / 1e6 / hbm, 4),
+                                     "exact": "bit-exact (the reference's double summed-area table, 8 B/element "
+                                              "scratch written and re-read per axis)"}
+    del x, s, o, ws
     # config 5: 4-D video 1024x1024x3x96, sigma (2.5, 2.5, -, 1.5), Reflect
     for name, dt in (("video_bf16", torch.bfloat16), ("video_f16", torch.float16), ("video_f32", torch.float32)):
         v = torch.rand((96, 3, 1024, 1024), generator=g, device="cuda", dtype=torch.float32)

@@ -147,6 +147,20 @@ NDLGPU_API ndlgpu_status ndlgpu_convolve_ex(const ndlgpu_view* src, const ndlgpu
  * The reference's default border is Reflect. */
 NDLGPU_API ndlgpu_status ndlgpu_gradient(const ndlgpu_view* src, const ndlgpu_view* dst, int border, void* stream);
 
+/* ndl::box_blur(src, dst, radius, border) -- processing/summed_area_table.h:300-339.
+ * The (2 radius + 1)^DIM box average through a summed-area table in double,
+ * built and queried exactly as the reference does (border-mapped padding,
+ * sequential running sums per axis, inclusion-exclusion over the 2^DIM
+ * corners, then sum / (2r+1)^DIM and DstT's static_cast), so the results
+ * equal the reference's bit for bit.  radius > 0; Wrap/Reflect need radius
+ * <= every extent.  The table (8 bytes per element of the padded extent)
+ * lives in `workspace` (at least ndlgpu_box_blur_workspace_size() bytes) or,
+ * with workspace NULL, in stream-ordered scratch. */
+NDLGPU_API ndlgpu_status ndlgpu_box_blur(const ndlgpu_view* src, const ndlgpu_view* dst, int radius, int border,
+                                         void* workspace, size_t workspace_bytes, void* stream);
+NDLGPU_API ndlgpu_status ndlgpu_box_blur_workspace_size(const ndlgpu_view* src, const ndlgpu_view* dst, int radius,
+                                                        int border, size_t* bytes);
+
 /* ndl::downsample(src, factor, channelAxis, border) -- processing/convolution.h:241-305.
  * Every axis but channel_axis shrinks to (extent - 1) / factor + 1 (dst must
  * have those extents; the reference returns a new image of them); each

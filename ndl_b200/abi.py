@@ -91,6 +91,8 @@ SIGNATURES = {
     "ndlgpu_gradient": (_I, [_PV, _PV, _I, _VP]),
     "ndlgpu_dog_scale_space": (_I, [_PV, _I, ctypes.c_double, _PV, _PV, _VP]),
     "ndlgpu_downsample": (_I, [_PV, _PV, _I, _I, _I, _VP]),
+    "ndlgpu_box_blur": (_I, [_PV, _PV, _I, _I, _VP, ctypes.c_size_t, _VP]),
+    "ndlgpu_box_blur_workspace_size": (_I, [_PV, _PV, _I, _I, ctypes.POINTER(ctypes.c_size_t)]),
     "ndlgpu_gaussian_blur": (_I, [_PV, _PV, ctypes.c_double, _I, _VP, _SZ, _VP]),
     "ndlgpu_gaussian_blur_workspace_size": (_I, [_PV, _PV, ctypes.c_double, _I, ctypes.POINTER(_SZ)]),
     "ndlgpu_gaussian_blur_axes": (_I, [_PV, _PV, ctypes.POINTER(ctypes.c_double), _I, _VP, _SZ, _VP]),

@@ -72,6 +72,28 @@ def gradient(src: Image, dst: Image = None, border=BorderMode.Reflect, stream=No
     return dst
 
 
+def box_blur(src: Image, dst: Image, radius: int, border=BorderMode.Clamp, workspace=None, stream=None):
+    """ndl::box_blur(src, dst, radius, border)
+    (processing/summed_area_table.h:300-339): the (2r+1)^DIM box average
+    through the reference's own summed-area-table arithmetic (bit-exact)."""
+    lib = abi.load()
+    sv, dv = src.abi_view(), dst.abi_view()
+    ws, wsb = _ws(workspace)
+    abi.check(lib.ndlgpu_box_blur(ctypes.byref(sv), ctypes.byref(dv), int(radius), int(border), ws, wsb,
+                                  _stream_ptr(stream)))
+    return dst
+
+
+def box_blur_workspace_size(src: Image, dst: Image, radius: int, border=BorderMode.Clamp):
+    """Bytes of the summed-area table box_blur needs (8 per padded element)."""
+    lib = abi.load()
+    sv, dv = src.abi_view(), dst.abi_view()
+    b = ctypes.c_size_t(0)
+    abi.check(lib.ndlgpu_box_blur_workspace_size(ctypes.byref(sv), ctypes.byref(dv), int(radius), int(border),
+                                                 ctypes.byref(b)))
+    return b.value
+
+
 def downsample(src: Image, factor: int, channel_axis=0, border=BorderMode.Clamp, dst: Image = None, stream=None):
     """ndl::downsample(src, factor, channelAxis, border)
     (processing/convolution.h:241-305): every axis but channel_axis shrinks

@@ -1891,6 +1891,72 @@ ndlgpu_status ndlgpu_dog_scale_space(const ndlgpu_view* src, int num_scales, dou
     return NDLGPU_OK;
 }
 
+static ndlgpu_status box_prepare(const ndlgpu_view* src, const ndlgpu_view* dst, int radius, int border, BoxParams* p)
+{
+    ndlgpu_status st;
+    if ((st = check_view(src, "src", true)) != NDLGPU_OK) return st;
+    if ((st = check_view(dst, "dst", true)) != NDLGPU_OK) return st;
+    if ((st = check_pair(src, dst)) != NDLGPU_OK) return st;
+    if (radius < 1) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "radius must be > 0 (summed_area_table.h:306)");
+    if (border < NDLGPU_CLAMP || border > NDLGPU_REFLECT) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "unknown border mode");
+    *p = BoxParams{};
+    p->rank = src->rank;
+    p->radius = radius;
+    p->border = border;
+    p->npad = 1;
+    p->total = view_count(src);
+    p->area = 1.0;
+    __int128 npad = 1;
+    for (int a = 0; a < src->rank; a++) {
+        if (border != NDLGPU_CLAMP && radius > src->extent[a] && src->extent[a] > 0)
+            return fail(NDLGPU_ERR_RADIUS_EXCEEDS_EXTENT, "Wrap/Reflect map one period: radius must not exceed extent " +
+                                                               std::to_string(src->extent[a]) + " (mathHelpers.h:23-24)");
+        p->ext[a] = (int)src->extent[a];
+        p->sstr[a] = src->stride[a];
+        p->dstr[a] = dst->stride[a];
+        p->pext[a] = src->extent[a] + 2 * (int64_t)radius;
+        p->pst[a] = (int64_t)npad;
+        npad *= p->pext[a];
+        p->area *= (2 * radius + 1);
+    }
+    if (npad > ((__int128)1 << 40)) return fail(NDLGPU_ERR_INDEX_OVERFLOW, "padded summed-area table too large");
+    p->npad = (int64_t)npad;
+    p->src = static_cast<const char*>(src->data);
+    p->dst = static_cast<char*>(dst->data);
+    p->sdt = src->dtype;
+    p->ddt = dst->dtype;
+    return NDLGPU_OK;
+}
+
+ndlgpu_status ndlgpu_box_blur_workspace_size(const ndlgpu_view* src, const ndlgpu_view* dst, int radius, int border,
+                                             size_t* bytes)
+{
+    t_last_error.clear();
+    if (!bytes) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "bytes is NULL");
+    BoxParams p;
+    ndlgpu_status st = box_prepare(src, dst, radius, border, &p);
+    if (st != NDLGPU_OK) return st;
+    *bytes = p.total == 0 ? 0 : align_up((size_t)p.npad * sizeof(double));
+    return NDLGPU_OK;
+}
+
+ndlgpu_status ndlgpu_box_blur(const ndlgpu_view* src, const ndlgpu_view* dst, int radius, int border, void* workspace,
+                              size_t workspace_bytes, void* stream)
+{
+    // ndl::box_blur (processing/summed_area_table.h:300-339)
+    t_last_error.clear();
+    BoxParams p;
+    ndlgpu_status st = box_prepare(src, dst, radius, border, &p);
+    if (st != NDLGPU_OK || p.total == 0) return st;
+    Scratch sc;
+    const cudaStream_t s = (cudaStream_t)stream;
+    if ((st = get_scratch(align_up((size_t)p.npad * sizeof(double)), workspace, workspace_bytes, s, &sc)) != NDLGPU_OK)
+        return st;
+    p.table = static_cast<double*>(sc.base);
+    cudaError_t e = launch_box_blur(p, s);
+    return e == cudaSuccess ? NDLGPU_OK : cuda_fail(e, "box_blur launch");
+}
+
 ndlgpu_status ndlgpu_downsample(const ndlgpu_view* src, const ndlgpu_view* dst, int factor, int channel_axis,
                                 int border, void* stream)
 {

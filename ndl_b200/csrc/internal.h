@@ -310,6 +310,24 @@ struct DownParams {
 };
 cudaError_t launch_downsample(const DownParams& p, cudaStream_t s);
 
+// box_blur (boxblur.cu): the reference's summed-area-table arithmetic.
+struct BoxParams {
+    const char* src;
+    char* dst;
+    int sdt, ddt;
+    int rank;
+    int radius;
+    int border;
+    int ext[kMaxRank];
+    int64_t sstr[kMaxRank], dstr[kMaxRank];
+    int64_t pext[kMaxRank], pst[kMaxRank];   // padded extents and the table's strides
+    int64_t npad;                            // table elements
+    int64_t total;                           // outputs
+    double area;                             // (2r+1)^DIM
+    double* table;
+};
+cudaError_t launch_box_blur(const BoxParams& p, cudaStream_t s);
+
 // Batched form (batch.cu): one persistent launch over a table of instances.
 constexpr int kBatchMaxTaps = 37;
 struct BatchDesc {

@@ -350,3 +350,77 @@ int ora_downsample(int dim, const double* src, const int64_t* ext, const int64_t
     }
     return 0;
 }
+
+/*
+ * box_blur(src, dst, radius, border) -- processing/summed_area_table.h:300-339.
+ * 1. A padded copy of extent ext + 2r per axis, each position p holding the
+ *    source value at the border-mapped p - r (:319-322).
+ * 2. Its summed-area table in double (:48-88): the values, then one running
+ *    sum per axis in axis order, each fiber summed from index 0 upward.
+ * 3. Per output, rectangle_sum() over [c, c + 2r] (:117-137): the 2^DIM
+ *    corners in mask order (bit i set: corner0[i] - 1 on axis i, sign
+ *    flipped), corners with a negative coordinate skipped, each term
+ *    sign * table added to the running total; then total / (2r+1)^DIM.
+ * Writes the double quotients (the DstT static_cast is ora_cast's).
+ * src is read through strides; out is contiguous (axis 0 fastest).
+ */
+int ora_box_blur(int dim, const double* src, const int64_t* ext, const int64_t* sstr, int radius, int border,
+                 double* out)
+{
+    if (dim < 1 || dim > 16 || radius < 1) return -1;
+    int64_t pext[16], pst[16], c[16];
+    int64_t np = 1;
+    for (int a = 0; a < dim; a++) {
+        pext[a] = ext[a] + 2 * radius;
+        pst[a] = np;
+        np *= pext[a];
+    }
+    double* t = (double*)malloc((size_t)np * sizeof(double));
+    if (!t) return -2;
+    for (int a = 0; a < dim; a++) c[a] = 0;
+    for (int64_t i = 0; i < np; i++) {
+        int64_t off = 0;
+        for (int a = 0; a < dim; a++) off += ora_map(border, ext[a], c[a] - radius) * sstr[a];
+        t[i] = src[off];
+        ora_next(dim, pext, c);
+    }
+    for (int axis = 0; axis < dim; axis++) {
+        for (int a = 0; a < dim; a++) c[a] = 0;
+        for (int64_t i = 0; i < np; i++) {
+            if (c[axis] == 0) {
+                int64_t off = 0;
+                for (int a = 0; a < dim; a++) off += c[a] * pst[a];
+                double running = 0.0;
+                for (int64_t k = 0; k < pext[axis]; k++) {
+                    running = running + t[off + k * pst[axis]];
+                    t[off + k * pst[axis]] = running;
+                }
+            }
+            ora_next(dim, pext, c);
+        }
+    }
+    double area = 1.0;
+    for (int a = 0; a < dim; a++) area *= (2 * radius + 1);
+    const int64_t n = ora_count(dim, ext);
+    for (int a = 0; a < dim; a++) c[a] = 0;
+    for (int64_t i = 0; i < n; i++) {
+        double total = 0.0;
+        for (int mask = 0; mask < (1 << dim); mask++) {
+            int sign = 1, oob = 0;
+            int64_t off = 0;
+            for (int a = 0; a < dim; a++) {
+                const int low = (mask >> a) & 1;
+                const int64_t q = low ? c[a] - 1 : c[a] + 2 * radius;
+                if (low) sign = -sign;
+                if (q < 0) { oob = 1; break; }
+                off += q * pst[a];
+            }
+            if (oob) continue;
+            total = total + sign * t[off];
+        }
+        out[i] = total / area;
+        ora_next(dim, ext, c);
+    }
+    free(t);
+    return 0;
+}

@@ -55,7 +55,8 @@ def _load():
         if not os.path.exists(path):
             raise RuntimeError("oracle not built: run oracle/build_oracle.py")
         _lib = ctypes.CDLL(path)
-        for name in ("ora_convolve", "ora_axis_pass", "ora_axis_pass_adjoint", "ora_axis_tap_grad", "ora_downsample"):
+        for name in ("ora_convolve", "ora_axis_pass", "ora_axis_pass_adjoint", "ora_axis_tap_grad", "ora_downsample",
+                     "ora_box_blur"):
             getattr(_lib, name).restype = ctypes.c_int
         _lib.ora_gaussian_weights.restype = ctypes.c_int
         _lib.ora_gaussian_weights.argtypes = [ctypes.c_double, _f64p]
@@ -82,7 +83,7 @@ def _load_ref():
             raise RuntimeError("reference shim not built (oracle/build_oracle.py needs the ndl source tree)")
         _ref = ctypes.CDLL(reference_path())
         for name in ("ref_convolve", "ref_gaussian_blur", "ref_compose", "ref_view_probe", "ref_gradient",
-                     "ref_detect_keypoints", "ref_downsample", "ref_per_channel_blur"):
+                     "ref_detect_keypoints", "ref_downsample", "ref_per_channel_blur", "ref_box_blur"):
             getattr(_ref, name).restype = ctypes.c_int
     return _ref
 
@@ -301,6 +302,20 @@ def downsample(src, factor, channel_axis=0, code=None, out_code=None):
     return cast(out, dtype_code(src, code) if out_code is None else out_code, STORE_ROUND)
 
 
+def box_blur(src, radius, border=CLAMP, out_code=None, code=None):
+    """box_blur(src, dst, radius, border), processing/summed_area_table.h:
+    300-339: the reference's summed-area-table arithmetic in double, then a
+    static_cast to DstT (truncation for integral types)."""
+    x = to_f64(src, code)
+    ext, st = _ndl_geom(x)
+    out = np.zeros(x.shape, np.float64)
+    rc = _load().ora_box_blur(x.ndim, x.ctypes.data_as(_f64p), _arr64(ext), _arr64(st), int(radius), int(border),
+                              out.ctypes.data_as(_f64p))
+    if rc != 0:
+        raise RuntimeError("ora_box_blur failed")
+    return cast(out, dtype_code(src, code) if out_code is None else out_code, STORE_CAST)
+
+
 def dog_sigmas(num_scales, sigma0):
     """sigma_i = sigma0 * 2^(i / (num_scales - 3)), feature_detection.h:105-107."""
     return [sigma0 * 2.0 ** (i / (num_scales - 3)) for i in range(num_scales)]
@@ -436,6 +451,19 @@ def ref_per_channel_blur(src, sigma, channel_axis, border=CLAMP):
                                   ctypes.c_void_p(out.ctypes.data))
     if rc != 0:
         raise RuntimeError("ref_per_channel_blur failed (%d)" % rc)
+    return out
+
+
+def ref_box_blur(src, radius, border=CLAMP, out_dtype=None):
+    """Runs ndl::box_blur() itself."""
+    lib = _load_ref()
+    out = np.zeros(src.shape, out_dtype or src.dtype)
+    ext, sst = _ndl_geom(src)
+    _, dst = _ndl_geom(out)
+    rc = lib.ref_box_blur(src.ndim, dtype_code(src), ctypes.c_void_p(src.ctypes.data), _i32arr(ext), _i32arr(sst),
+                          dtype_code(out), ctypes.c_void_p(out.ctypes.data), _i32arr(dst), int(radius), int(border))
+    if rc != 0:
+        raise RuntimeError("ref_box_blur failed (%d)" % rc)
     return out
 
 

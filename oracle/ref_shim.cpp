@@ -18,6 +18,7 @@
 #include <ndl/image.h>
 #include <ndl/processing/convolution.h>
 #include <ndl/processing/feature_detection.h>
+#include <ndl/processing/summed_area_table.h>
 
 #include <array>
 #include <cstdint>
@@ -144,6 +145,25 @@ int ref_per_channel_blur(int dim, int tsrc, void* src, const int* ext, int chann
                 return 0;
             });
         }
+    });
+}
+
+// ndl::box_blur(src, dst, radius, border) (processing/summed_area_table.h:300-339).
+int ref_box_blur(int dim, int tsrc, void* src, const int* ext, const int* sstr, int tdst, void* dst, const int* dstr,
+                 int radius, int border)
+{
+    return dispatch_dim(dim, [&](auto D) {
+        constexpr int DIM = decltype(D)::value;
+        return dispatch_type(tsrc, [&](auto s) {
+            using S = decltype(s);
+            return dispatch_type(tdst, [&](auto d) {
+                using Dt = decltype(d);
+                auto sv = make_view<S, DIM>(src, ext, sstr);
+                auto dv = make_view<Dt, DIM>(dst, ext, dstr);
+                ndl::box_blur(sv, dv, radius, to_border(border));
+                return 0;
+            });
+        });
     });
 }
 

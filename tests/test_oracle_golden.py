@@ -265,3 +265,21 @@ def test_per_channel_blur_oracle_matches_compiled_reference(shape, ch):
         x = (rng.random(shape) * 200).astype(dt)
         for b in (0, 1, 2):
             assert (O.ref_per_channel_blur(x, 1.3, ch, b) == O.per_channel_blur(x, 1.3, ch, b)).all(), (dt, b)
+
+
+@pytest.mark.skipif(not O.have_reference(), reason="compiled reference not present")
+@pytest.mark.parametrize("shape", [(17,), (20, 23), (9, 10, 11), (5, 6, 7, 4)])
+def test_box_blur_oracle_matches_compiled_reference(shape):
+    """box_blur (summed_area_table.h:300-339): padded copy, double table
+    built axis by axis, corner inclusion-exclusion, then the cast -- bit for
+    bit, floating types included (the running sums keep the reference's
+    order)."""
+    rng = np.random.default_rng(len(shape))
+    for dt, odt in [(np.uint8, np.uint8), (np.float32, np.float32), (np.float64, np.float64), (np.int16, np.float32)]:
+        x = (rng.random(shape) * 200).astype(dt) if dt != np.float64 else rng.standard_normal(shape)
+        for r in (1, 2, 3):
+            for b in (0, 1, 2):
+                if r > min(shape) and b != 0:
+                    continue
+                ref = O.ref_box_blur(x, r, b, odt)
+                assert (ref == O.box_blur(x, r, b, O.dtype_code(np.zeros(1, odt)))).all(), (dt, r, b)
