@@ -135,6 +135,32 @@ void gaussian_blur(const SrcImageT& src, DstImageT& dst, double sigma, BorderT b
     detail::check(ndlgpu_gaussian_blur(&s, &d, sigma, static_cast<int>(border), workspace, workspace_bytes, stream));
 }
 
+/// ndl::box_blur on device memory (processing/summed_area_table.h:300-339):
+/// the (2 radius + 1)^DIM box average through the reference's own
+/// summed-area-table arithmetic (bit-exact).  Scratch as for gaussian_blur
+/// (see ndlgpu_box_blur_workspace_size).
+template <class SrcImageT, class DstImageT, class BorderT = int>
+void box_blur(const SrcImageT& src, DstImageT& dst, int radius, BorderT border = BorderT(0), void* stream = nullptr,
+              void* workspace = nullptr, size_t workspace_bytes = 0)
+{
+    const ndlgpu_view s = detail::view_of(src);
+    const ndlgpu_view d = detail::view_of(dst);
+    detail::check(ndlgpu_box_blur(&s, &d, radius, static_cast<int>(border), workspace, workspace_bytes, stream));
+}
+
+/// ndl::downsample on device memory (processing/convolution.h:241-305).  The
+/// reference returns a new image; here the caller passes dst with the
+/// decimated extents ((extent - 1) / factor + 1 on every axis but
+/// channelAxis).  Bit-exact block averages.
+template <class SrcImageT, class DstImageT, class BorderT = int>
+void downsample(const SrcImageT& src, DstImageT& dst, int factor, int channelAxis = 0, BorderT border = BorderT(0),
+                void* stream = nullptr)
+{
+    const ndlgpu_view s = detail::view_of(src);
+    const ndlgpu_view d = detail::view_of(dst);
+    detail::check(ndlgpu_downsample(&s, &d, factor, channelAxis, static_cast<int>(border), stream));
+}
+
 }  // namespace ndlgpu
 
 #endif /* NDLGPU_DROPIN_H */
