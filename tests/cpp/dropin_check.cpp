@@ -6,6 +6,7 @@
 // and exits non-zero on any failure.
 #include <ndl/image.h>
 #include <ndl/processing/convolution.h>
+#include <ndl/processing/summed_area_table.h>
 
 #include <cuda_runtime.h>
 
@@ -138,7 +139,52 @@ int main()
         cudaFree(du);
         cudaFree(d16);
     }
-    // 4. the reference asserts on mismatched extents; the drop-in throws
+    // 4. box_blur (float view, Reflect) and downsample (uint8 colour image),
+    //    against ndl::box_blur and ndl::downsample themselves, bit-exact
+    {
+        const int NX = 70, NY = 45;
+        std::vector<float> fb((size_t)NX * NY);
+        std::uniform_real_distribution<float> u(0.f, 1.f);
+        for (auto& v : fb) v = u(rng);
+        ndl::Image<float, 2> hf(fb.data(), {NX, NY});
+        auto hv = hf.swap_axes(0, 1).mirror(0);
+        ndl::OwnedImage<float, 2> ref(hv.extent());
+        ndl::box_blur(hv, ref, 3, ndl::BorderMode::Reflect);
+        float* df = upload(fb);
+        ndl::Image<float, 2> gf(df, {NX, NY});
+        auto gv = gf.swap_axes(0, 1).mirror(0);
+        std::vector<float> got((size_t)NX * NY, 0.f);
+        float* dg = upload(got);
+        ndl::Image<float, 2> gg(dg, hv.extent());
+        ndlgpu::box_blur(gv, gg, 3, ndl::BorderMode::Reflect);
+        cudaMemcpy(got.data(), dg, got.size() * sizeof(float), cudaMemcpyDeviceToHost);
+        size_t bad = 0, i = 0;
+        for (const auto& c : ref.coordinates()) bad += (got[i++] != ref.at(c));
+        report("box_blur f32 view swap_axes(0,1).mirror(0) Reflect r=3, bit-exact", bad == 0, (double)bad);
+
+        const int W = 37, H = 23;
+        std::vector<uint8_t> rgb((size_t)3 * W * H);
+        for (auto& v : rgb) v = (uint8_t)(rng() & 255);
+        ndl::Image<uint8_t, 3> hc(rgb.data(), {3, W, H});
+        auto small = ndl::downsample(hc, 3);
+        uint8_t* dc = upload(rgb);
+        ndl::Image<uint8_t, 3> gc(dc, {3, W, H});
+        const auto es = small.extent();
+        std::vector<uint8_t> got8((size_t)es[0] * es[1] * es[2], 0);
+        uint8_t* ds = upload(got8);
+        ndl::Image<uint8_t, 3> gs(ds, es);
+        ndlgpu::downsample(gc, gs, 3);
+        cudaMemcpy(got8.data(), ds, got8.size(), cudaMemcpyDeviceToHost);
+        bad = 0;
+        i = 0;
+        for (const auto& c : small.coordinates()) bad += (got8[i++] != small.at(c));
+        report("downsample u8 {3, 37, 23} by 3, bit-exact", bad == 0, (double)bad);
+        cudaFree(df);
+        cudaFree(dg);
+        cudaFree(dc);
+        cudaFree(ds);
+    }
+    // 5. the reference asserts on mismatched extents; the drop-in throws
     {
         float* d = nullptr;
         cudaMalloc(&d, 64 * sizeof(float));
