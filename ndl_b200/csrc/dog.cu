@@ -12,8 +12,9 @@
 // pairs; lanes of a warp take consecutive rows, conflict-free on the odd
 // pitch), then the Y pass (2 columns x 4 rows per thread, packed), keeps the
 // level in registers and writes level - previous level.  Both passes keep
-// their sample window in slots indexed by tap mod 4 (an unrolled-by-4 tap
-// loop), so no value is ever moved between registers.  The
+// their sample window in slots indexed by tap mod 4 (a tap loop unrolled by
+// 4, the last K mod 4 taps guarded), so no value is ever moved between
+// registers.  The
 // source is read once instead of num_scales times, and no level goes through
 // HBM unless the caller asks for it.
 //
@@ -120,15 +121,24 @@ __global__ void __launch_bounds__(DNT, 2) k_dog2d(const __grid_constant__ DogPar
             wv[3] = make_float2(0.f, 0.f);
             float2 a[4] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f),
                            make_float2(0.f, 0.f)};
-            for (int k = 0; k < K; k += 4) {
+            int k = 0;
+            for (; k + 4 <= K; k += 4) {
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
-                    if (k + q < K) {
-                        wv[(q + 3) & 3] = make_float2(s0[k + q + 3], s1[k + q + 3]);
-                        const float2 wk = w2[k + q];
+                    wv[(q + 3) & 3] = make_float2(s0[k + q + 3], s1[k + q + 3]);
+                    const float2 wk = w2[k + q];
 #pragma unroll
-                        for (int m = 0; m < 4; m++) a[m] = __ffma2_rn(wv[(q + m) & 3], wk, a[m]);
-                    }
+                    for (int m = 0; m < 4; m++) a[m] = __ffma2_rn(wv[(q + m) & 3], wk, a[m]);
+                }
+            }
+            // the last K mod 4 taps, the same slots
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+                if (k + q < K) {
+                    wv[(q + 3) & 3] = make_float2(s0[k + q + 3], s1[k + q + 3]);
+                    const float2 wk = w2[k + q];
+#pragma unroll
+                    for (int m = 0; m < 4; m++) a[m] = __ffma2_rn(wv[(q + m) & 3], wk, a[m]);
                 }
             }
             *reinterpret_cast<float4*>(s_x + i * XP + 4 * g) = make_float4(a[0].x, a[1].x, a[2].x, a[3].x);
@@ -145,15 +155,23 @@ __global__ void __launch_bounds__(DNT, 2) k_dog2d(const __grid_constant__ DogPar
             v[1] = *reinterpret_cast<const float2*>(xp + XP);
             v[2] = *reinterpret_cast<const float2*>(xp + 2 * XP);
             v[3] = make_float2(0.f, 0.f);
-            for (int k = 0; k < K; k += 4) {
+            int k = 0;
+            for (; k + 4 <= K; k += 4) {
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
-                    if (k + q < K) {
-                        v[(q + 3) & 3] = *reinterpret_cast<const float2*>(xp + (k + q + 3) * XP);
-                        const float2 wk = w2[k + q];
+                    v[(q + 3) & 3] = *reinterpret_cast<const float2*>(xp + (k + q + 3) * XP);
+                    const float2 wk = w2[k + q];
 #pragma unroll
-                        for (int j = 0; j < 4; j++) cur[j] = __ffma2_rn(v[(q + j) & 3], wk, cur[j]);
-                    }
+                    for (int j = 0; j < 4; j++) cur[j] = __ffma2_rn(v[(q + j) & 3], wk, cur[j]);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+                if (k + q < K) {
+                    v[(q + 3) & 3] = *reinterpret_cast<const float2*>(xp + (k + q + 3) * XP);
+                    const float2 wk = w2[k + q];
+#pragma unroll
+                    for (int j = 0; j < 4; j++) cur[j] = __ffma2_rn(v[(q + j) & 3], wk, cur[j]);
                 }
             }
         }
