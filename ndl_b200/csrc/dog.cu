@@ -10,7 +10,7 @@
 // float) into shared memory, then per level runs the X pass over the rows
 // that level's Y pass needs (one unit = 2 rows x 4 outputs as packed FP32
 // pairs; lanes of a warp take consecutive rows, conflict-free on the odd
-// pitch), then the Y pass (2 columns x 4 rows per thread, packed), keeps the
+// pitch), then the Y pass (2 columns x DTY/8 rows per thread, packed), keeps the
 // level in registers and writes level - previous level.  Both passes keep
 // their sample window in slots indexed by tap mod 4 (a tap loop unrolled by
 // 4, the last K mod 4 taps guarded), so no value is ever moved between
@@ -30,7 +30,8 @@ namespace {
 
 constexpr int DTX = 64;     // outputs per tile along x
 constexpr int DTY = 32;     // outputs per tile along y
-constexpr int DNT = 256;    // threads: Y pass = 64 columns x 4 groups of 8 rows
+constexpr int DNT = 256;    // threads: Y pass = 32 column pairs x 8 row groups
+constexpr int RPT = DTY / (DNT / 32);   // Y-pass rows per thread (window slots)
 constexpr int XP = DTX + 4; // pitch of the X-pass buffer (float4 row stores spread over the banks)
 
 // Reflect (mathHelpers.h:24) for the coordinates an output inside the image
@@ -93,13 +94,13 @@ __global__ void __launch_bounds__(DNT, 2) k_dog2d(const __grid_constant__ DogPar
     }
     __syncthreads();
 
-    // Y-pass outputs of this thread: columns cx, cx+1 of rows ry .. ry+3
+    // Y-pass outputs of this thread: columns cx, cx+1 of rows ry .. ry+RPT-1
     const int cx = 2 * lane;
-    const int ry = 4 * warp;
+    const int ry = RPT * warp;
     const int ox = x0 + cx;
-    float2 prev[4];
+    float2 prev[RPT];
 #pragma unroll
-    for (int j = 0; j < 4; j++) prev[j] = make_float2(0.f, 0.f);
+    for (int j = 0; j < RPT; j++) prev[j] = make_float2(0.f, 0.f);
 
     for (int s = 0; s < p.ns; s++) {
         const int r = p.r[s];
@@ -145,33 +146,34 @@ __global__ void __launch_bounds__(DNT, 2) k_dog2d(const __grid_constant__ DogPar
             *reinterpret_cast<float4*>(s_x + (i + H) * XP + 4 * g) = make_float4(a[0].y, a[1].y, a[2].y, a[3].y);
         }
         __syncthreads();
-        // Y pass: (column cx, column cx+1) pairs down rows ry .. ry+3 with
-        // the same slot rotation
-        float2 cur[4] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+        // Y pass: (column cx, column cx+1) pairs down rows ry .. ry+RPT-1,
+        // window slot m holding row k+m (mod RPT)
+        float2 cur[RPT];
+#pragma unroll
+        for (int j = 0; j < RPT; j++) cur[j] = make_float2(0.f, 0.f);
         {
             const float* xp = s_x + ry * XP + cx;
-            float2 v[4];
-            v[0] = *reinterpret_cast<const float2*>(xp);
-            v[1] = *reinterpret_cast<const float2*>(xp + XP);
-            v[2] = *reinterpret_cast<const float2*>(xp + 2 * XP);
-            v[3] = make_float2(0.f, 0.f);
-            int k = 0;
-            for (; k + 4 <= K; k += 4) {
+            float2 v[RPT];
 #pragma unroll
-                for (int q = 0; q < 4; q++) {
-                    v[(q + 3) & 3] = *reinterpret_cast<const float2*>(xp + (k + q + 3) * XP);
+            for (int j = 0; j + 1 < RPT; j++) v[j] = *reinterpret_cast<const float2*>(xp + j * XP);
+            v[RPT - 1] = make_float2(0.f, 0.f);
+            int k = 0;
+            for (; k + RPT <= K; k += RPT) {
+#pragma unroll
+                for (int q = 0; q < RPT; q++) {
+                    v[(q + RPT - 1) % RPT] = *reinterpret_cast<const float2*>(xp + (k + q + RPT - 1) * XP);
                     const float2 wk = w2[k + q];
 #pragma unroll
-                    for (int j = 0; j < 4; j++) cur[j] = __ffma2_rn(v[(q + j) & 3], wk, cur[j]);
+                    for (int j = 0; j < RPT; j++) cur[j] = __ffma2_rn(v[(q + j) % RPT], wk, cur[j]);
                 }
             }
 #pragma unroll
-            for (int q = 0; q < 3; q++) {
+            for (int q = 0; q + 1 < RPT; q++) {
                 if (k + q < K) {
-                    v[(q + 3) & 3] = *reinterpret_cast<const float2*>(xp + (k + q + 3) * XP);
+                    v[(q + RPT - 1) % RPT] = *reinterpret_cast<const float2*>(xp + (k + q + RPT - 1) * XP);
                     const float2 wk = w2[k + q];
 #pragma unroll
-                    for (int j = 0; j < 4; j++) cur[j] = __ffma2_rn(v[(q + j) & 3], wk, cur[j]);
+                    for (int j = 0; j < RPT; j++) cur[j] = __ffma2_rn(v[(q + j) % RPT], wk, cur[j]);
                 }
             }
         }
@@ -180,7 +182,7 @@ __global__ void __launch_bounds__(DNT, 2) k_dog2d(const __grid_constant__ DogPar
             float* lv = p.lv[s];
             float* dg = s > 0 ? p.dg[s - 1] : nullptr;
 #pragma unroll
-            for (int j = 0; j < 4; j++) {
+            for (int j = 0; j < RPT; j++) {
                 const int oy = y0 + ry + j;
                 if (oy >= p.ny) break;
                 if (lv) store_pair(lv, p.lx[s], p.ly[s], p.lvec[s], ox, oy, p.nx, cur[j]);
@@ -190,7 +192,7 @@ __global__ void __launch_bounds__(DNT, 2) k_dog2d(const __grid_constant__ DogPar
             }
         }
 #pragma unroll
-        for (int j = 0; j < 4; j++) prev[j] = cur[j];
+        for (int j = 0; j < RPT; j++) prev[j] = cur[j];
     }
 }
 
