@@ -57,3 +57,18 @@ def test_box_blur_rejects_bad_calls():
     with pytest.raises(abi.NdlGpuError) as e:
         n.box_blur(src, dst, 2, 0, workspace=torch.empty(16, dtype=torch.uint8, device="cuda"))
     assert e.value.status == abi.ERR_WORKSPACE
+
+
+@pytest.mark.parametrize("dt", [np.uint8, np.float32])
+def test_box_blur_clamp_radius_beyond_extent_and_empty(dt):
+    """Clamp needs no period: a window wider than the image repeats the edge
+    samples (the reference pads with kernelTapCoord's clamp); empty images
+    are a no-op."""
+    rng = np.random.default_rng(11)
+    x = (rng.random((3, 40)) * 200).astype(dt)
+    src = Image.from_tensor(torch.from_numpy(x).cuda())
+    dst = Image.empty(src.extent(), src.dtype)
+    n.box_blur(src, dst, 5, 0)
+    assert (dst.tensor().cpu().numpy() == O.box_blur(x, 5, 0)).all()
+    e = Image.from_tensor(torch.zeros((0, 7), dtype=torch.float32, device="cuda"))
+    n.box_blur(e, Image.empty(e.extent(), torch.float32), 2, 2)

@@ -142,3 +142,9 @@ def test_dog_rejects_bad_calls():
     with pytest.raises(abi.NdlGpuError) as e:
         n.dog_scale_space(src, 4, -1.0)
     assert e.value.status == abi.ERR_BAD_SIGMA
+
+
+def test_dog_empty_image_is_a_no_op():
+    src = Image.from_tensor(torch.zeros((0, 64), device="cuda"))
+    dogs, levels = n.dog_scale_space(src, 5, 1.6, levels=True)
+    assert len(dogs) == 4 and len(levels) == 5

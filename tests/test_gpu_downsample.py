@@ -78,3 +78,15 @@ def test_per_channel_blur(shape, ch, dt):
             assert (got == ref).all(), b
         else:
             assert (np.abs(got.astype(np.float64) - ref) <= 1e-6 * np.abs(ref) + 1e-30).all(), b
+
+
+def test_downsample_factor_beyond_extent_and_empty():
+    """A factor larger than an axis leaves one output averaging the whole
+    axis; an empty source is a no-op."""
+    rng = np.random.default_rng(12)
+    x = (rng.random((4, 3, 2)) * 255).astype(np.uint8)          # ndl {2, 3, 4}, channel axis 0
+    out = n.downsample(Image.from_tensor(torch.from_numpy(x).cuda()), 5, 0)
+    assert out.extent() == [2, 1, 1]
+    assert (out.tensor().cpu().numpy() == O.downsample(x, 5, 0)).all()
+    e = Image.from_tensor(torch.zeros((0, 6, 3), dtype=torch.uint8, device="cuda"))
+    n.downsample(e, 2, 0)
