@@ -62,3 +62,70 @@ def test_two_rank_gloo_partition_and_job_time():
     assert sorted(mine0 + mine1) == list(range(len(costs))) and not set(mine0) & set(mine1)
     expect = max(sum(costs[i] for i in mine0), sum(costs[i] for i in mine1)) / 1e6
     assert abs(t0 - expect) < 1e-9 and abs(t1 - expect) < 1e-9
+
+
+# -- slabs of one volume along its slowest axis: the halo exchange ----------
+
+def _halo_worker(rank, world, port, vol, r, border, q):
+    import torch.distributed as dist
+    from ndl_b200.shard import exchange_halo, slab_bounds
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        a, b = slab_bounds(vol.shape[0], world, rank)
+        ext = exchange_halo(vol[a:b].clone(), r, border)
+        q.put((rank, a, b, ext.numpy()))          # by value: outlives this process
+    finally:
+        dist.destroy_process_group()
+
+
+def _expected_halo(vol, a, b, r, border):
+    """The extended slab built directly from the whole volume with the
+    border maps of mathHelpers.h:23-25."""
+    import torch
+    n = vol.shape[0]
+    idx = []
+    for t in range(a - r, b + r):
+        if 0 <= t < n:
+            idx.append(t)
+        elif border == 1:                               # Wrap
+            idx.append(t + n if t < 0 else t - n)
+        elif border == 2:                               # Reflect
+            idx.append(-t - 1 if t < 0 else 2 * n - t - 1)
+        else:                                           # Clamp
+            idx.append(0 if t < 0 else n - 1)
+    return vol[torch.tensor(idx)]
+
+
+@pytest.mark.parametrize("world", [2, 3])
+@pytest.mark.parametrize("border", [0, 1, 2])
+def test_slab_halo_exchange_gloo(world, border):
+    """Every rank's extended slab equals the volume's planes (border-mapped
+    beyond its ends), for 2 ranks (each the other's neighbour on both sides
+    under Wrap) and 3."""
+    import torch
+    vol = torch.arange(14 * 3 * 2, dtype=torch.float32).reshape(14, 3, 2)
+    r = 3
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_halo_worker, args=(k, world, port, vol, r, border, q)) for k in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=120) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, a, b, ext in res:
+        assert torch.equal(torch.from_numpy(ext), _expected_halo(vol, a, b, r, border)), (rank, border)
+
+
+def test_slab_bounds_and_single_rank_halo():
+    import torch
+    from ndl_b200.shard import exchange_halo, slab_bounds
+    spans = [slab_bounds(10, 3, k) for k in range(3)]
+    assert spans == [(0, 4), (4, 7), (7, 10)]
+    vol = torch.arange(6, dtype=torch.float32).reshape(6, 1)
+    for border in (0, 1, 2):
+        assert torch.equal(exchange_halo(vol, 2, border), _expected_halo(vol, 0, 6, 2, border))
