@@ -482,6 +482,17 @@ def other_forms(args, hbm):
                                  "gbs": round(16.0 * vox / ms / 1e6, 1),
                                  "frac_of_measured_hbm": round(16.0 * vox / ms / 1e6 / hbm, 4)}
     del x, s, o
+    # gaussian_blur of a 256^3 f32 volume (one sigma on every axis, Reflect)
+    # at sigma 1, 2 and 3: the fused 3-pass kernels of 7, 13 and 19 taps
+    x = torch.rand((256, 256, 256), generator=g, device="cuda")
+    s = Image.from_tensor(x)
+    o = Image.empty(s.extent(), torch.float32)
+    for sg in (1.0, 2.0, 3.0):
+        ms = time_call(lambda: n.gaussian_blur(s, o, sg, BorderMode.Reflect), it)
+        out["gaussian_blur_f32_256^3_sigma%g" % sg] = {
+            "ms": round(ms, 4), "gvoxel_s": round(x.numel() / ms / 1e6, 2), "gbs": round(8.0 * x.numel() / ms / 1e6, 1),
+            "frac_of_measured_hbm": round(8.0 * x.numel() / ms / 1e6 / hbm, 4)}
+    del x, s, o
     out["dog_f32_4096^2_5scales"] = dog_form(g, it, hbm)
     # downsample (convolution.h:241-305): a {3, 15360, 8640} uint8 colour
     # image (channel axis 0, 398 MB) by 2; algorithmic bytes = source + result

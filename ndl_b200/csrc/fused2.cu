@@ -170,7 +170,6 @@ struct Geo {
     static constexpr int MAXEL = ROWS * PITCH;
     static constexpr size_t TAB_BYTES = (size_t)MAXEL * 8;
     static constexpr size_t SMEM = IN_BYTES + X_BYTES + TAB_BYTES + 16 + 128;   // + alignment slack
-    static_assert(STAGE_BYTES % 128 == 0, "plane stages stay 128-byte aligned for the copy engine");
 };
 
 // Output plane sum of the Z queue for the newest slot S: tap k reads slot
@@ -224,7 +223,7 @@ __device__ __forceinline__ void zdispatch(int slot, float2 (&q)[KZ][4], const fl
 // CTAs per SM: the adjoint's border-zone paths need more registers.
 template <int TY, bool ADJ, int KZ>
 struct Occ {
-    static constexpr int value = TY <= 16 ? ((ADJ && KZ > 9) ? 3 : 4) : 2;
+    static constexpr int value = TY <= 16 ? (KZ > 11 ? 2 : ((ADJ && KZ > 9) ? 3 : 4)) : 2;
 };
 
 // TMA: plane loads through the tensor map (adjoint with zero padding only).
@@ -235,6 +234,7 @@ __global__ void __launch_bounds__(8 * TY, (Occ<TY, ADJ, KZ>::value))
     using G = Geo<Tin, KX, KY, TY>;
     constexpr int NT = G::NT;
     static_assert(!TMA || ADJ, "the copy-engine loader serves the zero-padded adjoint");
+    static_assert(!TMA || G::STAGE_BYTES % 128 == 0, "plane stages stay 128-byte aligned for the copy engine");
     extern __shared__ __align__(128) unsigned char smem_dyn[];
     __shared__ uint64_t s_bar[STAGES];
     unsigned char* smem_raw = smem_dyn + ((128u - (smem_u32(smem_dyn) & 127u)) & 127u);
@@ -645,6 +645,14 @@ struct Variant2 {
 #define NDLGPU_V2(A, TI, TO, DI, DO, KX_, KY_, KZ_, TY_) \
     {A, DI, DO, KX_, KY_, KZ_, &launch2<TI, TO, KX_, KY_, KZ_, TY_, (A != 0)>}
 const Variant2 kVariants2[] = {
+    // gaussian_blur of volumes: one width per radius 2..9 (sigma 0.5 .. 3)
+    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 5, 5, 5, 16),
+    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 7, 7, 7, 16),
+    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 11, 11, 11, 16),
+    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 13, 13, 13, 16),
+    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 15, 15, 15, 16),
+    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 17, 17, 17, 16),
+    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 19, 19, 19, 16),
     NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 9, 9, 9, 16),
     NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 13, 13, 1, 24),
     NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 17, 17, 11, 16),
