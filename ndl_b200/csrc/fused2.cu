@@ -655,6 +655,17 @@ const Variant2 kVariants2[] = {
     NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 19, 19, 19, 16),
     NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 9, 9, 9, 16),
     NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 13, 13, 1, 24),
+    // gaussian_blur of 2-D images: every width from radius 2 to 12 (sigma 0.5 to 4)
+    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 5, 5, 1, 24),
+    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 7, 7, 1, 24),
+    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 9, 9, 1, 24),
+    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 11, 11, 1, 24),
+    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 15, 15, 1, 24),
+    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 17, 17, 1, 24),
+    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 19, 19, 1, 24),
+    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 21, 21, 1, 24),
+    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 23, 23, 1, 24),
+    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 25, 25, 1, 24),
     NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 17, 17, 11, 16),
     NDLGPU_V2(0, __nv_bfloat16, __nv_bfloat16, NDLGPU_BF16, NDLGPU_BF16, 17, 17, 11, 16),
     NDLGPU_V2(0, __half, __half, NDLGPU_F16, NDLGPU_F16, 17, 17, 11, 16),
