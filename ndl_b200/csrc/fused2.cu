@@ -611,7 +611,9 @@ cudaError_t launch2(const FusedParams& p, cudaStream_t s)
     std::memset(&tmap, 0, sizeof(tmap));
     bool tma = false;
     auto kern = k_fused2<Tin, Tout, KX, KY, KZ, TY, ADJ, false>;
-    if constexpr (ADJ) {
+    // the copy engine writes 128-byte aligned stages: geometries whose plane
+    // stage is not a multiple of 128 bytes keep cp.async
+    if constexpr (ADJ && G::STAGE_BYTES % 128 == 0) {
         tma = plane_map<Tin>(pp, G::PITCH, G::ROWS, &tmap);
         if (tma) kern = k_fused2<Tin, Tout, KX, KY, KZ, TY, ADJ, true>;
     }
@@ -645,7 +647,10 @@ struct Variant2 {
 #define NDLGPU_V2(A, TI, TO, DI, DO, KX_, KY_, KZ_, TY_) \
     {A, DI, DO, KX_, KY_, KZ_, &launch2<TI, TO, KX_, KY_, KZ_, TY_, (A != 0)>}
 const Variant2 kVariants2[] = {
-    // gaussian_blur of volumes: one width per radius 2..9 (sigma 0.5 .. 3)
+    // small learnable filters (3 taps per axis) and gaussian_blur of volumes:
+    // one width per radius 1..9 (sigma 0.5 .. 3)
+    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 3, 3, 3, 16),
+    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 3, 3, 1, 24),
     NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 5, 5, 5, 16),
     NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 7, 7, 7, 16),
     NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 11, 11, 11, 16),
@@ -670,6 +675,14 @@ const Variant2 kVariants2[] = {
     NDLGPU_V2(0, __nv_bfloat16, __nv_bfloat16, NDLGPU_BF16, NDLGPU_BF16, 17, 17, 11, 16),
     NDLGPU_V2(0, __half, __half, NDLGPU_F16, NDLGPU_F16, 17, 17, 11, 16),
     NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 9, 9, 9, 16),
+    // input gradients of small filters (3, 5, 7 taps per axis; images up to 9)
+    NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 3, 3, 3, 16),
+    NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 5, 5, 5, 16),
+    NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 7, 7, 7, 16),
+    NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 3, 3, 1, 24),
+    NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 5, 5, 1, 24),
+    NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 7, 7, 1, 24),
+    NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 9, 9, 1, 24),
     NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 13, 13, 1, 24),
     NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 17, 17, 11, 16),
     NDLGPU_V2(1, __nv_bfloat16, __nv_bfloat16, NDLGPU_BF16, NDLGPU_BF16, 17, 17, 11, 16),

@@ -503,3 +503,36 @@ def test_gaussian_blur_image_fused_sigmas(sigma, border):
         ref = O.gaussian_blur(logical, sigma, border, O.F64)
         got = o.tensor().cpu().numpy().astype(np.float64)
         assert (np.abs(got - ref) <= 1e-6 * np.abs(ref) + 1e-30).all()
+
+
+@pytest.mark.parametrize("k", [3, 5, 7, 9])
+@pytest.mark.parametrize("border", [0, 1, 2])
+@pytest.mark.parametrize("shape", [(21, 34, 70), (2, 45, 67)])
+def test_small_filter_forward_and_input_gradient(k, border, shape):
+    """Small learnable filters: forward and dL/dX of k taps per axis on
+    volumes (3 passes) and on batches of 2-D images (2 passes; the leading
+    axis untouched), the fused kernels, against the FP64 oracle."""
+    rng = np.random.default_rng(k + 10 * border + len(shape))
+    two_d = shape[0] == 2
+    if not two_d and k == 9:
+        pytest.skip("9x9x9 is covered by the configuration-3 tests")
+    x = rand_array(rng, shape, np.float32)
+    g = rand_array(rng, shape, np.float32)
+    axes = (0, 1) if two_d else (0, 1, 2)
+    passes = []
+    for ax in axes:
+        w = rng.standard_normal(k)
+        passes.append((ax, w / np.abs(w).sum()))
+    y = Image.empty(list(shape[::-1]), torch.float32)
+    n.convolve_axes(Image.from_tensor(dev(x)), y, passes, border)
+    ref = O.compose_total(x, passes, border)
+    mag = O.compose_total(np.abs(x.astype(np.float64)), [(a, np.abs(w)) for a, w in passes], border)
+    assert_close(host(y.tensor()), ref, mag, 1e-6, "forward k=%d %s" % (k, shape))
+    gxi = Image.empty(list(shape[::-1]), torch.float32)
+    n.convolve_axes_adjoint(Image.from_tensor(dev(g)), None, gxi, passes, border, None)
+    gcur = g.astype(np.float64)
+    gmag = np.abs(gcur)
+    for ax, w in passes[::-1]:
+        gcur = O.axis_pass_adjoint(gcur, ax, w, border)
+        gmag = O.axis_pass_adjoint(gmag, ax, np.abs(w), border)
+    assert_close(host(gxi.tensor()), gcur, gmag, 1e-6, "adjoint k=%d %s" % (k, shape))
