@@ -39,7 +39,7 @@ def _needs_scratch(src, dst, sigma, border):
 
 @pytest.mark.parametrize("dtype,shape,sigma,border", [
     (torch.uint8, (37, 50, 61), 1.5, BorderMode.Reflect),      # exact double chain: two double volumes
-    (torch.float32, (200, 300), 1.1, BorderMode.Wrap),         # FP32 chain of two passes
+    (torch.float32, (200, 300), 4.5, BorderMode.Wrap),         # FP32 chain of two 29-tap passes (no fused width)
     (torch.float64, (90, 110), 2.0, BorderMode.Clamp),         # double chain, one intermediate
 ])
 def test_noalloc_matches_allocating_entry_point(dtype, shape, sigma, border):
