@@ -220,10 +220,11 @@ __device__ __forceinline__ void zdispatch(int slot, float2 (&q)[KZ][4], const fl
 #undef NDLGPU_ZCASE
 }
 
-// CTAs per SM: the adjoint's border-zone paths need more registers.
+// CTAs per SM: the adjoint's border-zone paths and deep Z queues need more
+// registers (13 planes fit 3 CTAs; 15 planes measured faster at 2).
 template <int TY, bool ADJ, int KZ>
 struct Occ {
-    static constexpr int value = TY <= 16 ? (KZ > 11 ? 2 : ((ADJ && KZ > 9) ? 3 : 4)) : 2;
+    static constexpr int value = TY <= 16 ? (KZ > 13 ? 2 : (KZ > 11 ? 3 : ((ADJ && KZ > 9) ? 3 : 4))) : 2;
 };
 
 // TMA: plane loads through the tensor map (adjoint with zero padding only).
