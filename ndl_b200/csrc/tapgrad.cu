@@ -68,25 +68,27 @@ struct TGeo {
     static constexpr int EPC = 16 / (int)sizeof(T);
     static constexpr int CX = KX / 2;
     static constexpr int CY = KY / 2;
-    static constexpr int D = (EPC - CX % EPC) % EPC;
-    static_assert(D == 0, "the tap-gradient kernel needs K/2 to be a multiple of the 16-byte element count");
+    static constexpr int D = (EPC - CX % EPC) % EPC;       // shared column of global x0 - CX
+    static constexpr int WBASE = (D / 4) * 4;               // first column of a 4-aligned window
+    static constexpr int WOFF = D % 4;                      // window offset inside it
     static constexpr int ROWS = TY + KY - 1;
-    static constexpr int XC = TX + KX - 1;                 // columns of Py X
-    static_assert(XC % 4 == 0, "K-1 must be a multiple of 4");
+    static constexpr int XC = TX + KX - 1;                 // columns of Py X the taps need
+    static constexpr int XCP = (WOFF + XC + 3) / 4 * 4;    // columns computed, from shared column WBASE
     static_assert(TY % 4 == 0, "the Y-pass units cover 4 rows");
-    static constexpr int NCH = (XC + EPC - 1) / EPC;
-    static constexpr int NV = (KX + 3 + 3) / 4;
-    static constexpr int WEND = 60 + 4 * NV;
+    static constexpr int NCH = (XC + D + EPC - 1) / EPC;
+    static constexpr int NV = (WOFF + KX + 3 + 3) / 4;
+    static constexpr int WEND0 = 60 + WBASE + 4 * NV;      // columns an X window reads
+    static constexpr int WEND = WEND0 > WBASE + XCP ? WEND0 : WBASE + XCP;   // and the Py X pass
     static constexpr int PITCH = (NCH * EPC > WEND ? NCH * EPC : (WEND + EPC - 1) / EPC * EPC);
     static constexpr int NTASK = (ROWS * NCH + NT - 1) / NT;
     static constexpr int NXU = ROWS * 16;                  // X-pass units: 1 row x 4 columns
-    static constexpr int NQ = XC / 4;
+    static constexpr int NQ = XCP / 4;
     static constexpr int NU = NXU + (TY / 4) * NQ;         // + Y-pass units: 4 rows x 4 columns
     static constexpr int NUR = (NU + NT - 1) / NT;          // unit rounds per thread
     static_assert((TY / 4) * NQ <= NT, "one Y unit per thread at most");
     static constexpr size_t IN_BYTES = (size_t)STAGES * ROWS * PITCH * sizeof(T);
     static constexpr size_t X1_BYTES = (size_t)ROWS * TX * 4;
-    static constexpr size_t X1Y_BYTES = (size_t)(TY * XC + 16) * 4;   // the last windows read past the end
+    static constexpr size_t X1Y_BYTES = (size_t)(TY * XCP + 16) * 4;   // the last windows read past the end
     static constexpr size_t TAB_BYTES = (size_t)ROWS * PITCH * 8;
     static constexpr size_t RED_BYTES = (size_t)(NT / 32) * 64 * 8;
     static constexpr size_t SMEM = IN_BYTES + X1_BYTES + X1Y_BYTES + TAB_BYTES + RED_BYTES + 16;
@@ -193,7 +195,7 @@ __global__ void __launch_bounds__(NT, 2) k_tapgrad(const __grid_constant__ TapFu
 
     if (zs < ze) {
         // X loader set-up (border-mapped halos, as the forward)
-        const int gx0 = x0 - G::CX;
+        const int gx0 = x0 - G::CX - G::D;   // global column of shared column 0 (16-byte aligned)
         if (tid == 0) *s_ntab = 0;
         __syncthreads();
         int32_t goff[G::NTASK];
@@ -310,13 +312,13 @@ __global__ void __launch_bounds__(NT, 2) k_tapgrad(const __grid_constant__ TapFu
                     const int r = (tid >> 4) + i * (NT / 16), g = tid & 15;
                     float win[G::NV * 4];
 #pragma unroll
-                    for (int v = 0; v < G::NV; v++) lds4(sb + r * G::PITCH + 4 * g + 4 * v, win + 4 * v);
+                    for (int v = 0; v < G::NV; v++) lds4(sb + r * G::PITCH + 4 * g + G::WBASE + 4 * v, win + 4 * v);
                     float a[4];
 #pragma unroll
                     for (int m = 0; m < 4; m++) {
                         float s = 0.f;
 #pragma unroll
-                        for (int k = 0; k < KX; k++) s = fmaf(win[m + k], p.wxf[k], s);
+                        for (int k = 0; k < KX; k++) s = fmaf(win[G::WOFF + m + k], p.wxf[k], s);
                         a[m] = s;
                     }
                     *reinterpret_cast<float4*>(s_x1 + r * TX + 4 * g) = make_float4(a[0], a[1], a[2], a[3]);
@@ -324,7 +326,7 @@ __global__ void __launch_bounds__(NT, 2) k_tapgrad(const __grid_constant__ TapFu
                     // Py X: 4 rows x 4 columns, each loaded row feeding up to
                     // 4 outputs (packed FMA over column pairs)
                     const int rg = y_rg, qq = y_qq;
-                    const T* col = sb + (4 * rg) * G::PITCH + 4 * qq;
+                    const T* col = sb + (4 * rg) * G::PITCH + G::WBASE + 4 * qq;
                     float2 a[4][2];
 #pragma unroll
                     for (int h = 0; h < 4; h++) a[h][0] = a[h][1] = make_float2(0.f, 0.f);
@@ -344,7 +346,7 @@ __global__ void __launch_bounds__(NT, 2) k_tapgrad(const __grid_constant__ TapFu
                     }
 #pragma unroll
                     for (int h = 0; h < 4; h++)
-                        *reinterpret_cast<float4*>(s_x1y + (4 * rg + h) * G::XC + 4 * qq) =
+                        *reinterpret_cast<float4*>(s_x1y + (4 * rg + h) * G::XCP + 4 * qq) =
                             make_float4(a[h][0].x, a[h][0].y, a[h][1].x, a[h][1].y);
                 }
             }
@@ -373,10 +375,11 @@ __global__ void __launch_bounds__(NT, 2) k_tapgrad(const __grid_constant__ TapFu
             {
                 float win[G::NV * 4];
 #pragma unroll
-                for (int v = 0; v < G::NV; v++) lds4(s_x1y + gyq * G::XC + 4 * gxq + 4 * v, win + 4 * v);
+                for (int v = 0; v < G::NV; v++) lds4(s_x1y + gyq * G::XCP + 4 * gxq + 4 * v, win + 4 * v);
 #pragma unroll
                 for (int k = 0; k < KX; k++)
-                    dwx[k] = fmaf(g2[0], win[k], fmaf(g2[1], win[k + 1], fmaf(g2[2], win[k + 2], fmaf(g2[3], win[k + 3], dwx[k]))));
+                    dwx[k] = fmaf(g2[0], win[G::WOFF + k], fmaf(g2[1], win[G::WOFF + k + 1],
+                                  fmaf(g2[2], win[G::WOFF + k + 2], fmaf(g2[3], win[G::WOFF + k + 3], dwx[k]))));
             }
             // positions outside the image carry g2 = 0 but x2 from mapped
             // loads: zero x2 there so that dwz sees no contribution
@@ -461,6 +464,9 @@ struct TgVariant {
     TgFn fn;
 };
 const TgVariant kTg[] = {
+    {NDLGPU_F32, 3, 3, 3, &launch_tg<float, 3, 3, 3>},
+    {NDLGPU_F32, 5, 5, 5, &launch_tg<float, 5, 5, 5>},
+    {NDLGPU_F32, 7, 7, 7, &launch_tg<float, 7, 7, 7>},
     {NDLGPU_F32, 9, 9, 9, &launch_tg<float, 9, 9, 9>},
     {NDLGPU_F32, 17, 17, 9, &launch_tg<float, 17, 17, 9>},
     {NDLGPU_F32, 17, 17, 11, &launch_tg<float, 17, 17, 11>},

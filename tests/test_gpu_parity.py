@@ -556,3 +556,33 @@ def test_gaussian_blur_16bit_fused_widths(tdt, shape, sigmas):
             ref = O.gaussian_blur(decoded, sigma, border, O.F64)
             got = o.tensor().float().cpu().numpy().astype(np.float64)
             assert (np.abs(got - ref) <= 4e-3 * np.abs(ref) + 1e-30).all(), (sigma, border)
+
+
+@pytest.mark.parametrize("k", [3, 5, 7])
+@pytest.mark.parametrize("border", [0, 1, 2])
+def test_small_filter_tap_gradients(k, border):
+    """All 3k tap gradients of a k-tap-per-axis filter on a batch of volumes
+    (one fused pass over X and G; the window starts off the 16-byte grid),
+    through mirrored views, against the FP64 oracle's literal transpose."""
+    rng = np.random.default_rng(77 + 3 * k + border)
+    base = rng.standard_normal((2, 23, 37, 70)).astype(np.float32)      # (b, z, y, x)
+    g = rng.standard_normal((2, 23, 37, 70)).astype(np.float32)
+    taps = [rng.standard_normal(k) for _ in range(3)]
+    xi = Image.from_tensor(dev(base)).mirror(0).mirror(2)
+    npx = base[:, ::-1, :, ::-1]
+    passes = [(0, taps[0]), (1, taps[1]), (2, taps[2])]
+    tg = torch.zeros(3 * k, dtype=torch.float64, device=DEV)
+    gi = Image.from_tensor(dev(g))
+    gx = Image.empty(gi.extent(), torch.float32)
+    n.convolve_axes_adjoint(gi, xi, gx, passes, border, tg)
+    ref_gx, ref_t = [], []
+    for b in range(2):
+        a, t = O.compose_adjoint(g[b].astype(np.float64), np.ascontiguousarray(npx[b]).astype(np.float64), passes,
+                                 border)
+        ref_gx.append(a)
+        ref_t.append(np.concatenate(t))
+    tref = np.sum(ref_t, axis=0)
+    got = host(tg)
+    assert np.abs(got - tref).max() <= 2e-5 * np.abs(tref).max(), np.abs(got - tref).max() / np.abs(tref).max()
+    gref = np.stack(ref_gx)
+    assert np.abs(host(gx.tensor()) - gref).max() <= 2e-6 * np.abs(gref).max()
