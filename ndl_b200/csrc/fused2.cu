@@ -713,6 +713,8 @@ const Variant2 kVariants2[] = {
     NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 3, 3, 3, 16),
     NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 5, 5, 5, 16),
     NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 7, 7, 7, 16),
+    NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 11, 11, 11, 16),
+    NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 13, 13, 13, 16),
     NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 3, 3, 1, 24),
     NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 5, 5, 1, 24),
     NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 7, 7, 1, 24),

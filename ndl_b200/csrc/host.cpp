@@ -1160,7 +1160,9 @@ static ndlgpu_status adjoint_execute(const ndlgpu_view* g, const ndlgpu_view* x,
         int ndt;
         std::vector<int64_t> nst;
         if (p > 0) {
-            gnext = B[p % 2];
+            // the intermediates alternate between the nB = min(2, n - 1)
+            // buffers, the first pass (p = n - 1) writing B[0]
+            gnext = B[(n - 1 - p) % 2];
             ndt = adt;
             nst = cst;
         } else if (gx) {

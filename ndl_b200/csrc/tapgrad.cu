@@ -467,6 +467,8 @@ const TgVariant kTg[] = {
     {NDLGPU_F32, 3, 3, 3, &launch_tg<float, 3, 3, 3>},
     {NDLGPU_F32, 5, 5, 5, &launch_tg<float, 5, 5, 5>},
     {NDLGPU_F32, 7, 7, 7, &launch_tg<float, 7, 7, 7>},
+    {NDLGPU_F32, 11, 11, 11, &launch_tg<float, 11, 11, 11>},
+    {NDLGPU_F32, 13, 13, 13, &launch_tg<float, 13, 13, 13>},
     {NDLGPU_F32, 9, 9, 9, &launch_tg<float, 9, 9, 9>},
     {NDLGPU_F32, 17, 17, 9, &launch_tg<float, 17, 17, 9>},
     {NDLGPU_F32, 17, 17, 11, &launch_tg<float, 17, 17, 11>},

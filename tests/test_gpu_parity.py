@@ -505,7 +505,7 @@ def test_gaussian_blur_image_fused_sigmas(sigma, border):
         assert (np.abs(got - ref) <= 1e-6 * np.abs(ref) + 1e-30).all()
 
 
-@pytest.mark.parametrize("k", [3, 5, 7, 9])
+@pytest.mark.parametrize("k", [3, 5, 7, 9, 11, 13])
 @pytest.mark.parametrize("border", [0, 1, 2])
 @pytest.mark.parametrize("shape", [(21, 34, 70), (2, 45, 67)])
 def test_small_filter_forward_and_input_gradient(k, border, shape):
@@ -558,7 +558,7 @@ def test_gaussian_blur_16bit_fused_widths(tdt, shape, sigmas):
             assert (np.abs(got - ref) <= 4e-3 * np.abs(ref) + 1e-30).all(), (sigma, border)
 
 
-@pytest.mark.parametrize("k", [3, 5, 7])
+@pytest.mark.parametrize("k", [3, 5, 7, 11, 13])
 @pytest.mark.parametrize("border", [0, 1, 2])
 def test_small_filter_tap_gradients(k, border):
     """All 3k tap gradients of a k-tap-per-axis filter on a batch of volumes
