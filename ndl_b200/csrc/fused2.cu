@@ -709,7 +709,7 @@ const Variant2 kVariants2[] = {
     NDLGPU_V2(0, __half, __half, NDLGPU_F16, NDLGPU_F16, 25, 25, 1, 24),
     NDLGPU_V2(0, __half, __half, NDLGPU_F16, NDLGPU_F16, 17, 17, 11, 16),
     NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 9, 9, 9, 16),
-    // input gradients of small filters (3, 5, 7 taps per axis; images up to 9)
+    // input gradients of small filters (3-13 taps per axis on volumes, 3-17 on images)
     NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 3, 3, 3, 16),
     NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 5, 5, 5, 16),
     NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 7, 7, 7, 16),
@@ -719,6 +719,9 @@ const Variant2 kVariants2[] = {
     NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 5, 5, 1, 24),
     NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 7, 7, 1, 24),
     NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 9, 9, 1, 24),
+    NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 11, 11, 1, 24),
+    NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 15, 15, 1, 24),
+    NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 17, 17, 1, 24),
     NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 13, 13, 1, 24),
     NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 17, 17, 11, 16),
     NDLGPU_V2(1, __nv_bfloat16, __nv_bfloat16, NDLGPU_BF16, NDLGPU_BF16, 17, 17, 11, 16),

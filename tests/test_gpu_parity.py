@@ -586,3 +586,33 @@ def test_small_filter_tap_gradients(k, border):
     assert np.abs(got - tref).max() <= 2e-5 * np.abs(tref).max(), np.abs(got - tref).max() / np.abs(tref).max()
     gref = np.stack(ref_gx)
     assert np.abs(host(gx.tensor()) - gref).max() <= 2e-6 * np.abs(gref).max()
+
+
+@pytest.mark.parametrize("border", [0, 1, 2])
+def test_general_adjoint_two_passes(border):
+    """The general (non-fused) input and tap gradients of a two-pass chain:
+    a zero tap keeps the chain off the fused kernels, and two passes use one
+    intermediate buffer."""
+    rng = np.random.default_rng(90 + border)
+    shape = (3, 37, 52)                                  # a batch of 2-D images
+    x = rand_array(rng, shape, np.float32)
+    g = rand_array(rng, shape, np.float32)
+    w0 = rng.standard_normal(7)
+    w0[2] = 0.0
+    w1 = rng.standard_normal(5)
+    passes = [(0, w0), (1, w1)]
+    tg = torch.zeros(12, dtype=torch.float64, device=DEV)
+    gxi = Image.empty(list(shape[::-1]), torch.float32)
+    n.convolve_axes_adjoint(Image.from_tensor(dev(g)), Image.from_tensor(dev(x)), gxi, passes, border, tg)
+    gx_only = Image.empty(list(shape[::-1]), torch.float32)
+    n.convolve_axes_adjoint(Image.from_tensor(dev(g)), None, gx_only, passes, border, None)
+    ref_gx, ref_t = [], []
+    for b in range(3):
+        a, t = O.compose_adjoint(g[b].astype(np.float64), x[b].astype(np.float64), passes, border)
+        ref_gx.append(a)
+        ref_t.append(np.concatenate(t))
+    gref = np.stack(ref_gx)
+    tref = np.sum(ref_t, axis=0)
+    for got in (host(gxi.tensor()), host(gx_only.tensor())):
+        assert np.abs(got - gref).max() <= 2e-6 * np.abs(gref).max()
+    assert np.abs(host(tg) - tref).max() <= 2e-5 * np.abs(tref).max()
