@@ -966,7 +966,10 @@ static bool plan_fused_tapgrad(const ndlgpu_view* g, const ndlgpu_view* x, int n
 {
     if (!x || x->dtype != g->dtype) return false;
     if (x->dtype != NDLGPU_F32 && x->dtype != NDLGPU_BF16 && x->dtype != NDLGPU_F16) return false;
-    if (npass != 3) return false;
+    // three passes (volumes), or two (images: the planes the kernel streams
+    // are then an axis without a pass, run as a one-tap unit pass whose
+    // gradient is not reported)
+    if (npass != 3 && npass != 2) return false;
     const std::string keep = t_last_error;
     std::vector<LPass> lp;
     if (lpasses_from(npass, passes, &lp) != NDLGPU_OK) { t_last_error = keep; return false; }
@@ -974,7 +977,7 @@ static bool plan_fused_tapgrad(const ndlgpu_view* g, const ndlgpu_view* x, int n
     if (canonicalise(x, g, lp, border, &c, true) != NDLGPU_OK || c.total == 0) { t_last_error = keep; return false; }
     const int R = (int)c.ax.size();
     std::vector<int> pass_of(R, -1);
-    for (int i = 0; i < 3; i++) {
+    for (int i = 0; i < npass; i++) {
         if (pass_of[c.passes[i].axis] >= 0) return false;
         pass_of[c.passes[i].axis] = i;
     }
@@ -982,10 +985,16 @@ static bool plan_fused_tapgrad(const ndlgpu_view* g, const ndlgpu_view* x, int n
     std::vector<int> others;
     for (int i = 1; i < R; i++)
         if (pass_of[i] >= 0) others.push_back(i);
-    if (others.size() != 2) return false;
-    const int role[3] = {0, others[0], others[1]};
-    int K[3];
+    if ((int)others.size() != npass - 1) return false;
+    // images: Z is the first axis without a pass (-1: a single plane)
+    int zrole = npass == 3 ? others[1] : -1;
+    if (npass == 2)
+        for (int i = 1; i < R && zrole < 0; i++)
+            if (pass_of[i] < 0) zrole = i;
+    const int role[3] = {0, others[0], zrole};
+    int K[3] = {1, 1, 1};
     for (int r = 0; r < 3; r++) {
+        if (role[r] < 0 || pass_of[role[r]] < 0) continue;   // the unit pass
         std::vector<int> o = c.passes[pass_of[role[r]]].off;
         std::sort(o.begin(), o.end());
         const int k = (int)o.size();
@@ -1004,7 +1013,8 @@ static bool plan_fused_tapgrad(const ndlgpu_view* g, const ndlgpu_view* x, int n
     p.zero_pad = border != NDLGPU_WRAP;
     const CAxis& ax0 = c.ax[role[0]];
     const CAxis& ay = c.ax[role[1]];
-    const CAxis& az = c.ax[role[2]];
+    const CAxis unit{1, 0, 0, -1};
+    const CAxis& az = role[2] >= 0 ? c.ax[role[2]] : unit;
     p.nx = (int)ax0.n; p.ny = (int)ay.n; p.nz = (int)az.n;
     p.sx = ax0.ss; p.sy = ay.ss; p.sz = az.ss;
     p.gxs = ax0.ds; p.gy = ay.ds; p.gz = az.ds;
@@ -1030,11 +1040,17 @@ static bool plan_fused_tapgrad(const ndlgpu_view* g, const ndlgpu_view* x, int n
     size_t base[3] = {0, 0, 0};
     {
         size_t off = 0;
-        for (int i = 0; i < 3; i++) { base[i] = off; off += (size_t)passes[i].ntaps; }
+        for (int i = 0; i < npass; i++) { base[i] = off; off += (size_t)passes[i].ntaps; }
     }
     float* wdst[3] = {p.wxf, p.wyf, p.wzf};
     int t = 0;
     for (int r = 0; r < 3; r++) {
+        if (role[r] < 0 || pass_of[role[r]] < 0) {
+            // the unit pass of an image: weight 1, gradient discarded
+            wdst[r][0] = 1.f;
+            ft->map.dst[t++] = -1;
+            continue;
+        }
         const int pi = pass_of[role[r]];
         const CPass& cp = c.passes[pi];
         const int la = passes[pi].axis;

@@ -430,6 +430,7 @@ __global__ void k_tapgrad_final(const double* partial, int ncta, int ntap, TapFi
     for (int s = 16; s > 0; s >>= 1) a += __shfl_down_sync(0xffffffffu, a, s);
     if (lane == 0) {
         const int o = mp.dst[t];
+        if (o < 0) return;                 // an image's unit pass: not reported
         if (out_dtype == NDLGPU_F64) ((double*)out)[o] = a;
         else ((float*)out)[o] = (float)a;
     }
@@ -464,6 +465,13 @@ struct TgVariant {
     TgFn fn;
 };
 const TgVariant kTg[] = {
+    // images (two passes and a unit pass across the planes)
+    {NDLGPU_F32, 3, 3, 1, &launch_tg<float, 3, 3, 1>},
+    {NDLGPU_F32, 5, 5, 1, &launch_tg<float, 5, 5, 1>},
+    {NDLGPU_F32, 7, 7, 1, &launch_tg<float, 7, 7, 1>},
+    {NDLGPU_F32, 9, 9, 1, &launch_tg<float, 9, 9, 1>},
+    {NDLGPU_F32, 11, 11, 1, &launch_tg<float, 11, 11, 1>},
+    {NDLGPU_F32, 13, 13, 1, &launch_tg<float, 13, 13, 1>},
     {NDLGPU_F32, 3, 3, 3, &launch_tg<float, 3, 3, 3>},
     {NDLGPU_F32, 5, 5, 5, &launch_tg<float, 5, 5, 5>},
     {NDLGPU_F32, 7, 7, 7, &launch_tg<float, 7, 7, 7>},

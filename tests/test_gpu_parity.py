@@ -616,3 +616,32 @@ def test_general_adjoint_two_passes(border):
     for got in (host(gxi.tensor()), host(gx_only.tensor())):
         assert np.abs(got - gref).max() <= 2e-6 * np.abs(gref).max()
     assert np.abs(host(tg) - tref).max() <= 2e-5 * np.abs(tref).max()
+
+
+@pytest.mark.parametrize("k", [3, 5, 9, 13])
+@pytest.mark.parametrize("border", [0, 1, 2])
+@pytest.mark.parametrize("shape", [(3, 45, 70), (61, 83)])
+def test_image_filter_tap_gradients(k, border, shape):
+    """Tap gradients of a two-pass (image) filter through the fused kernel:
+    a batch of images streamed as planes, and a single image, with dL/dX in
+    the same call; against the FP64 oracle's literal transpose."""
+    rng = np.random.default_rng(300 + k + 5 * border + len(shape))
+    x = rng.standard_normal(shape).astype(np.float32)
+    g = rng.standard_normal(shape).astype(np.float32)
+    taps = [rng.standard_normal(k) for _ in range(2)]
+    passes = [(0, taps[0]), (1, taps[1])]
+    tg = torch.zeros(2 * k, dtype=torch.float64, device=DEV)
+    gi = Image.from_tensor(dev(g))
+    gx = Image.empty(gi.extent(), torch.float32)
+    n.convolve_axes_adjoint(gi, Image.from_tensor(dev(x)), gx, passes, border, tg)
+    xs = x if len(shape) == 3 else x[None]
+    gs = g if len(shape) == 3 else g[None]
+    ref_gx, ref_t = [], []
+    for b in range(xs.shape[0]):
+        a, t = O.compose_adjoint(gs[b].astype(np.float64), xs[b].astype(np.float64), passes, border)
+        ref_gx.append(a)
+        ref_t.append(np.concatenate(t))
+    tref = np.sum(ref_t, axis=0)
+    assert np.abs(host(tg) - tref).max() <= 2e-5 * np.abs(tref).max()
+    gref = np.stack(ref_gx).reshape(shape)
+    assert np.abs(host(gx.tensor()) - gref).max() <= 2e-6 * np.abs(gref).max()
