@@ -660,14 +660,15 @@ const Variant2 kVariants2[] = {
     NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 17, 17, 17, 16),
     NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 19, 19, 19, 16),
     NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 9, 9, 9, 16),
-    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 13, 13, 1, 24),
-    // gaussian_blur of 2-D images: every width from radius 2 to 12 (sigma 0.5 to 4)
-    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 5, 5, 1, 24),
-    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 7, 7, 1, 24),
-    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 9, 9, 1, 24),
-    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 11, 11, 1, 24),
-    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 15, 15, 1, 24),
-    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 17, 17, 1, 24),
+    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 13, 13, 1, 16),
+    // gaussian_blur of 2-D images: every width from radius 2 to 12 (sigma 0.5 to 4);
+    // 16-row tiles (4 CTAs per SM) up to 17 taps, 24-row tiles beyond (measured)
+    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 5, 5, 1, 16),
+    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 7, 7, 1, 16),
+    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 9, 9, 1, 16),
+    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 11, 11, 1, 16),
+    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 15, 15, 1, 16),
+    NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 17, 17, 1, 16),
     NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 19, 19, 1, 24),
     NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 21, 21, 1, 24),
     NDLGPU_V2(0, float, float, NDLGPU_F32, NDLGPU_F32, 23, 23, 1, 24),
