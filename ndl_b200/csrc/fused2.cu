@@ -681,13 +681,13 @@ const Variant2 kVariants2[] = {
     NDLGPU_V2(0, __nv_bfloat16, __nv_bfloat16, NDLGPU_BF16, NDLGPU_BF16, 9, 9, 9, 16),
     NDLGPU_V2(0, __nv_bfloat16, __nv_bfloat16, NDLGPU_BF16, NDLGPU_BF16, 11, 11, 11, 16),
     NDLGPU_V2(0, __nv_bfloat16, __nv_bfloat16, NDLGPU_BF16, NDLGPU_BF16, 13, 13, 13, 16),
-    NDLGPU_V2(0, __nv_bfloat16, __nv_bfloat16, NDLGPU_BF16, NDLGPU_BF16, 5, 5, 1, 24),
-    NDLGPU_V2(0, __nv_bfloat16, __nv_bfloat16, NDLGPU_BF16, NDLGPU_BF16, 7, 7, 1, 24),
-    NDLGPU_V2(0, __nv_bfloat16, __nv_bfloat16, NDLGPU_BF16, NDLGPU_BF16, 9, 9, 1, 24),
-    NDLGPU_V2(0, __nv_bfloat16, __nv_bfloat16, NDLGPU_BF16, NDLGPU_BF16, 11, 11, 1, 24),
-    NDLGPU_V2(0, __nv_bfloat16, __nv_bfloat16, NDLGPU_BF16, NDLGPU_BF16, 13, 13, 1, 24),
-    NDLGPU_V2(0, __nv_bfloat16, __nv_bfloat16, NDLGPU_BF16, NDLGPU_BF16, 15, 15, 1, 24),
-    NDLGPU_V2(0, __nv_bfloat16, __nv_bfloat16, NDLGPU_BF16, NDLGPU_BF16, 17, 17, 1, 24),
+    NDLGPU_V2(0, __nv_bfloat16, __nv_bfloat16, NDLGPU_BF16, NDLGPU_BF16, 5, 5, 1, 16),
+    NDLGPU_V2(0, __nv_bfloat16, __nv_bfloat16, NDLGPU_BF16, NDLGPU_BF16, 7, 7, 1, 16),
+    NDLGPU_V2(0, __nv_bfloat16, __nv_bfloat16, NDLGPU_BF16, NDLGPU_BF16, 9, 9, 1, 16),
+    NDLGPU_V2(0, __nv_bfloat16, __nv_bfloat16, NDLGPU_BF16, NDLGPU_BF16, 11, 11, 1, 16),
+    NDLGPU_V2(0, __nv_bfloat16, __nv_bfloat16, NDLGPU_BF16, NDLGPU_BF16, 13, 13, 1, 16),
+    NDLGPU_V2(0, __nv_bfloat16, __nv_bfloat16, NDLGPU_BF16, NDLGPU_BF16, 15, 15, 1, 16),
+    NDLGPU_V2(0, __nv_bfloat16, __nv_bfloat16, NDLGPU_BF16, NDLGPU_BF16, 17, 17, 1, 16),
     NDLGPU_V2(0, __nv_bfloat16, __nv_bfloat16, NDLGPU_BF16, NDLGPU_BF16, 19, 19, 1, 24),
     NDLGPU_V2(0, __nv_bfloat16, __nv_bfloat16, NDLGPU_BF16, NDLGPU_BF16, 21, 21, 1, 24),
     NDLGPU_V2(0, __nv_bfloat16, __nv_bfloat16, NDLGPU_BF16, NDLGPU_BF16, 23, 23, 1, 24),
@@ -697,13 +697,13 @@ const Variant2 kVariants2[] = {
     NDLGPU_V2(0, __half, __half, NDLGPU_F16, NDLGPU_F16, 9, 9, 9, 16),
     NDLGPU_V2(0, __half, __half, NDLGPU_F16, NDLGPU_F16, 11, 11, 11, 16),
     NDLGPU_V2(0, __half, __half, NDLGPU_F16, NDLGPU_F16, 13, 13, 13, 16),
-    NDLGPU_V2(0, __half, __half, NDLGPU_F16, NDLGPU_F16, 5, 5, 1, 24),
-    NDLGPU_V2(0, __half, __half, NDLGPU_F16, NDLGPU_F16, 7, 7, 1, 24),
-    NDLGPU_V2(0, __half, __half, NDLGPU_F16, NDLGPU_F16, 9, 9, 1, 24),
-    NDLGPU_V2(0, __half, __half, NDLGPU_F16, NDLGPU_F16, 11, 11, 1, 24),
-    NDLGPU_V2(0, __half, __half, NDLGPU_F16, NDLGPU_F16, 13, 13, 1, 24),
-    NDLGPU_V2(0, __half, __half, NDLGPU_F16, NDLGPU_F16, 15, 15, 1, 24),
-    NDLGPU_V2(0, __half, __half, NDLGPU_F16, NDLGPU_F16, 17, 17, 1, 24),
+    NDLGPU_V2(0, __half, __half, NDLGPU_F16, NDLGPU_F16, 5, 5, 1, 16),
+    NDLGPU_V2(0, __half, __half, NDLGPU_F16, NDLGPU_F16, 7, 7, 1, 16),
+    NDLGPU_V2(0, __half, __half, NDLGPU_F16, NDLGPU_F16, 9, 9, 1, 16),
+    NDLGPU_V2(0, __half, __half, NDLGPU_F16, NDLGPU_F16, 11, 11, 1, 16),
+    NDLGPU_V2(0, __half, __half, NDLGPU_F16, NDLGPU_F16, 13, 13, 1, 16),
+    NDLGPU_V2(0, __half, __half, NDLGPU_F16, NDLGPU_F16, 15, 15, 1, 16),
+    NDLGPU_V2(0, __half, __half, NDLGPU_F16, NDLGPU_F16, 17, 17, 1, 16),
     NDLGPU_V2(0, __half, __half, NDLGPU_F16, NDLGPU_F16, 19, 19, 1, 24),
     NDLGPU_V2(0, __half, __half, NDLGPU_F16, NDLGPU_F16, 21, 21, 1, 24),
     NDLGPU_V2(0, __half, __half, NDLGPU_F16, NDLGPU_F16, 23, 23, 1, 24),
