@@ -727,6 +727,15 @@ const Variant2 kVariants2[] = {
     NDLGPU_V2(1, float, float, NDLGPU_F32, NDLGPU_F32, 17, 17, 11, 16),
     NDLGPU_V2(1, __nv_bfloat16, __nv_bfloat16, NDLGPU_BF16, NDLGPU_BF16, 17, 17, 11, 16),
     NDLGPU_V2(1, __half, __half, NDLGPU_F16, NDLGPU_F16, 17, 17, 11, 16),
+    // 16-bit input gradients of small volume filters
+    NDLGPU_V2(1, __nv_bfloat16, __nv_bfloat16, NDLGPU_BF16, NDLGPU_BF16, 3, 3, 3, 16),
+    NDLGPU_V2(1, __nv_bfloat16, __nv_bfloat16, NDLGPU_BF16, NDLGPU_BF16, 5, 5, 5, 16),
+    NDLGPU_V2(1, __nv_bfloat16, __nv_bfloat16, NDLGPU_BF16, NDLGPU_BF16, 7, 7, 7, 16),
+    NDLGPU_V2(1, __nv_bfloat16, __nv_bfloat16, NDLGPU_BF16, NDLGPU_BF16, 9, 9, 9, 16),
+    NDLGPU_V2(1, __half, __half, NDLGPU_F16, NDLGPU_F16, 3, 3, 3, 16),
+    NDLGPU_V2(1, __half, __half, NDLGPU_F16, NDLGPU_F16, 5, 5, 5, 16),
+    NDLGPU_V2(1, __half, __half, NDLGPU_F16, NDLGPU_F16, 7, 7, 7, 16),
+    NDLGPU_V2(1, __half, __half, NDLGPU_F16, NDLGPU_F16, 9, 9, 9, 16),
 };
 #undef NDLGPU_V2
 

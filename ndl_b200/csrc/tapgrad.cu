@@ -480,6 +480,15 @@ const TgVariant kTg[] = {
     {NDLGPU_F32, 9, 9, 9, &launch_tg<float, 9, 9, 9>},
     {NDLGPU_F32, 17, 17, 9, &launch_tg<float, 17, 17, 9>},
     {NDLGPU_F32, 17, 17, 11, &launch_tg<float, 17, 17, 11>},
+    // 16-bit small volume filters
+    {NDLGPU_BF16, 3, 3, 3, &launch_tg<__nv_bfloat16, 3, 3, 3>},
+    {NDLGPU_BF16, 5, 5, 5, &launch_tg<__nv_bfloat16, 5, 5, 5>},
+    {NDLGPU_BF16, 7, 7, 7, &launch_tg<__nv_bfloat16, 7, 7, 7>},
+    {NDLGPU_BF16, 9, 9, 9, &launch_tg<__nv_bfloat16, 9, 9, 9>},
+    {NDLGPU_F16, 3, 3, 3, &launch_tg<__half, 3, 3, 3>},
+    {NDLGPU_F16, 5, 5, 5, &launch_tg<__half, 5, 5, 5>},
+    {NDLGPU_F16, 7, 7, 7, &launch_tg<__half, 7, 7, 7>},
+    {NDLGPU_F16, 9, 9, 9, &launch_tg<__half, 9, 9, 9>},
     {NDLGPU_BF16, 17, 17, 11, &launch_tg<__nv_bfloat16, 17, 17, 11>},
     {NDLGPU_F16, 17, 17, 11, &launch_tg<__half, 17, 17, 11>},
 };

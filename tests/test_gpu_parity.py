@@ -645,3 +645,35 @@ def test_image_filter_tap_gradients(k, border, shape):
     assert np.abs(host(tg) - tref).max() <= 2e-5 * np.abs(tref).max()
     gref = np.stack(ref_gx).reshape(shape)
     assert np.abs(host(gx.tensor()) - gref).max() <= 2e-6 * np.abs(gref).max()
+
+
+@pytest.mark.parametrize("tdt", [torch.bfloat16, torch.float16])
+@pytest.mark.parametrize("k", [3, 5, 7, 9])
+@pytest.mark.parametrize("border", [0, 2])
+def test_small_filter_gradients_16bit(tdt, k, border):
+    """16-bit storage of X, G and dL/dX for small volume filters: dL/dX within
+    4e-3 of the stencil magnitude, the tap gradients within 1e-4 of the
+    largest, both against the FP64 oracle on the decoded values."""
+    rng = np.random.default_rng(500 + k + border)
+    shape = (2, 21, 30, 70)
+    x = torch.from_numpy(rng.standard_normal(shape).astype(np.float32)).to(tdt)
+    g = torch.from_numpy(rng.standard_normal(shape).astype(np.float32)).to(tdt)
+    passes = [(a, rng.standard_normal(k)) for a in range(3)]
+    xi, gi = Image.from_tensor(x.cuda()), Image.from_tensor(g.cuda())
+    gx = Image.empty(gi.extent(), tdt)
+    tg = torch.zeros(3 * k, dtype=torch.float64, device=DEV)
+    n.convolve_axes_adjoint(gi, xi, gx, passes, border, tg)
+    xd, gd = x.float().numpy().astype(np.float64), g.float().numpy().astype(np.float64)
+    ref_gx, ref_t, mag = [], [], []
+    for b in range(2):
+        a, t = O.compose_adjoint(gd[b], xd[b], passes, border)
+        ref_gx.append(a)
+        ref_t.append(np.concatenate(t))
+        m = np.abs(gd[b])
+        for ax, w in passes[::-1]:
+            m = O.axis_pass_adjoint(m, ax, np.abs(w), border)
+        mag.append(m)
+    got = gx.tensor().float().cpu().numpy().astype(np.float64)
+    assert (np.abs(got - np.stack(ref_gx)) <= 4e-3 * np.stack(mag) + 1e-30).all()
+    tref = np.sum(ref_t, axis=0)
+    assert np.abs(host(tg) - tref).max() <= 1e-4 * np.abs(tref).max()
