@@ -1632,6 +1632,39 @@ ndlgpu_status ndlgpu_convolve_ex(const ndlgpu_view* src, const ndlgpu_view* dst,
     else if (precision == NDLGPU_PREC_AUTO && !dtype_integral(dst->dtype) && dst->dtype != NDLGPU_F64 &&
              src->dtype != NDLGPU_F64)
         acc = Acc::F32;
+    // f32 images with a dense 2-D / 3-D kernel of up to 9 taps per axis: the
+    // tiled stencil (stencil.cu)
+    if (acc == Acc::F32 && src->dtype == NDLGPU_F32 && dst->dtype == NDLGPU_F32 && (R == 2 || R == 3) &&
+        (int64_t)w.size() == kn) {
+        bool fits = true;
+        for (int i = 0; i < R; i++) fits = fits && kernel->extent[i] <= kStencilMaxTaps;
+        if (fits) {
+            StencilParams sp;
+            std::memset(&sp, 0, sizeof(sp));
+            sp.src = static_cast<const float*>(src->data);
+            sp.dst = static_cast<float*>(dst->data);
+            sp.nx = (int)src->extent[0];
+            sp.ny = (int)src->extent[1];
+            sp.nz = R == 3 ? (int)src->extent[2] : 1;
+            sp.nb = 1;
+            sp.sx = src->stride[0];
+            sp.sy = src->stride[1];
+            sp.sz = R == 3 ? src->stride[2] : 0;
+            sp.dx = dst->stride[0];
+            sp.dy = dst->stride[1];
+            sp.dz = R == 3 ? dst->stride[2] : 0;
+            sp.kx = (int)kernel->extent[0];
+            sp.ky = (int)kernel->extent[1];
+            sp.kz = R == 3 ? (int)kernel->extent[2] : 1;
+            sp.cx = sp.kx / 2;
+            sp.cy = sp.ky / 2;
+            sp.cz = sp.kz / 2;
+            sp.border = border;
+            for (size_t t = 0; t < w.size(); t++) sp.w[t] = (float)w[t];
+            cudaError_t e = launch_stencil(sp, (cudaStream_t)stream);
+            return e == cudaSuccess ? NDLGPU_OK : cuda_fail(e, "stencil launch");
+        }
+    }
     GenericNdParams p;
     std::memset(&p, 0, sizeof(p));
     p.src = (const char*)src->data;

@@ -677,3 +677,25 @@ def test_small_filter_gradients_16bit(tdt, k, border):
     assert (np.abs(got - np.stack(ref_gx)) <= 4e-3 * np.stack(mag) + 1e-30).all()
     tref = np.sum(ref_t, axis=0)
     assert np.abs(host(tg) - tref).max() <= 1e-4 * np.abs(tref).max()
+
+
+@pytest.mark.parametrize("kshape", [(3, 3), (4, 5), (7, 7), (2, 9), (3, 3, 3), (5, 4, 3), (1, 3, 5), (9, 2, 2)])
+@pytest.mark.parametrize("border", [0, 1, 2])
+def test_full_kernel_f32_stencil(kshape, border):
+    """convolve() with a dense (non-separable) kernel of up to 9 taps per
+    axis on f32 images and volumes: the tiled stencil, through a mirrored,
+    axis-swapped view, within 1e-6 of the stencil magnitude of the FP64
+    oracle (kernel shapes in numpy order: the last is ndl axis 0)."""
+    rng = np.random.default_rng(sum(kshape) * 7 + border)
+    shape = (77, 130) if len(kshape) == 2 else (19, 30, 45)
+    x = rng.standard_normal(shape).astype(np.float32)
+    k = rng.standard_normal(kshape)
+    k[np.abs(k) < 1e-3] = 0.5                       # dense: no zero tap
+    base = Image.from_tensor(dev(x))
+    src = base.swap_axes(0, 1).mirror(0)
+    logical = src.tensor().cpu().numpy()
+    o = Image.empty(src.extent(), torch.float32)
+    n.convolve(src, o, k, border)
+    ref = O.convolve_total(logical, k, border)
+    mag = O.convolve_total(np.abs(logical.astype(np.float64)), np.abs(k), border)
+    assert_close(host(o.tensor()), ref, mag, 1e-6, "stencil %s border %d" % (kshape, border))
