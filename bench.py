@@ -379,16 +379,48 @@ def time_call(fn, iters, warm=3, stream=None):
     return a.elapsed_time(b) / iters
 
 
+def fp64_blur_reference(v, sigmas):
+    """FP64 reference of gaussian_blur_axes with Reflect borders, in plain
+    PyTorch on the GPU: for each ndl axis with a sigma, the Gaussian taps of
+    ndl's formula (radius ceil(3 sigma), exp(-d^2 / (2 sigma^2)) normalised,
+    computed in double) applied as a correlation over the symmetric-reflect
+    extended axis (ndl's Reflect duplicates the edge sample)."""
+    import math
+
+    import torch
+
+    import ndl_b200 as n
+    x = v.double()
+    nd = x.dim()
+    for ax, sg in enumerate(sigmas):
+        if sg <= 0:
+            continue
+        r = n.gaussian_radius(sg)
+        w = [math.exp(-(d * d) / (2.0 * sg * sg)) for d in range(-r, r + 1)]
+        tot = sum(w)
+        w = [t / tot for t in w]
+        dim = nd - 1 - ax                          # ndl axis 0 is the last torch dim
+        m = x.shape[dim]
+        idx = torch.arange(-r, m + r, device=x.device)
+        idx = torch.where(idx < 0, -idx - 1, torch.where(idx >= m, 2 * m - idx - 1, idx))
+        ext = x.index_select(dim, idx)
+        acc = torch.zeros_like(x)
+        for k in range(2 * r + 1):
+            acc += w[k] * ext.narrow(dim, k, m)
+        x = acc
+    return x
+
+
 def video_error(dt, seed=SEED):
-    """Error of the configuration-5 blur in storage type dt against the FP64
-    oracle, on a 96 x 3 x 128 x 128 (t, c, y, x) crop with the same value
-    distribution (the GPU and the oracle see the same decoded inputs; data and
-    taps are positive, so the stencil magnitude is the exact result)."""
+    """Error of the configuration-5 blur in storage type dt against an FP64
+    reference (plain PyTorch in double on the same decoded inputs), on a
+    96 x 3 x 128 x 128 (t, c, y, x) crop with the same value distribution;
+    data and taps are positive, so the stencil magnitude is the exact
+    result."""
     import torch
 
     import ndl_b200 as n
     from ndl_b200 import BorderMode, Image
-    from oracle import oracle as O
 
     g = torch.Generator(device="cuda")
     g.manual_seed(seed + 5)
@@ -398,12 +430,11 @@ def video_error(dt, seed=SEED):
     o = Image.empty(Image.from_tensor(v).extent(), dt)
     sig = (2.5, 2.5, 0.0, 1.5)
     n.gaussian_blur_axes(Image.from_tensor(v), o, list(sig), BorderMode.Reflect)
-    got = o.tensor().float().cpu().numpy().astype(np.float64)
-    ref = O.compose_total(v.float().cpu().numpy().astype(np.float64),
-                          [(ax, O.gaussian_weights(sg)) for ax, sg in enumerate(sig) if sg > 0], O.REFLECT)
-    rel = np.abs(got - ref) / np.maximum(np.abs(ref), 1e-30)
+    ref = fp64_blur_reference(v.float(), sig)
+    got = o.tensor().double()
+    rel = ((got - ref).abs() / ref.abs().clamp_min(1e-30)).cpu().numpy()
     return {"max_rel": float("%.3g" % rel.max()), "rms_rel": float("%.3g" % np.sqrt((rel ** 2).mean())),
-            "sample": "96x3x128x128 crop, same distribution, vs FP64 oracle"}
+            "sample": "96x3x128x128 crop, same distribution, vs an FP64 PyTorch reference"}
 
 
 def dog_fma_per_pixel(num_scales, sigma0, tile_rows=32):
@@ -493,6 +524,33 @@ def other_forms(args, hbm):
             "ms": round(ms, 4), "gvoxel_s": round(x.numel() / ms / 1e6, 2), "gbs": round(8.0 * x.numel() / ms / 1e6, 1),
             "frac_of_measured_hbm": round(8.0 * x.numel() / ms / 1e6 / hbm, 4)}
     del x, s, o
+    # convolve() with a full (non-separable) 5x5 kernel on a 4096^2 f32 image
+    x = torch.rand((4096, 4096), generator=g, device="cuda")
+    s = Image.from_tensor(x)
+    o = Image.empty(s.extent(), torch.float32)
+    ker = np.random.default_rng(SEED).random((5, 5)) + 0.1
+    ms = time_call(lambda: n.convolve(s, o, ker, BorderMode.Reflect), it)
+    out["convolve_full5x5_f32_4096^2"] = {"ms": round(ms, 4), "gpixel_s": round(x.numel() / ms / 1e6, 2),
+                                          "gbs": round(8.0 * x.numel() / ms / 1e6, 1),
+                                          "frac_of_measured_hbm": round(8.0 * x.numel() / ms / 1e6 / hbm, 4)}
+    del x, s, o
+    # a learnable 3-tap-per-axis separable filter on eight 192^3 f32 volumes:
+    # forward, dL/dX and the 9 tap gradients of one training step
+    X = torch.randn((8, 192, 192, 192), generator=g, device="cuda")
+    W = torch.randn_like(X)
+    Y, GX = torch.empty_like(X), torch.empty_like(X)
+    T = torch.zeros(9, device="cuda")
+    xi, wi, yi, gi = (Image.from_tensor(t) for t in (X, W, Y, GX))
+    taps3 = [(a, np.random.default_rng(SEED + a).standard_normal(3)) for a in range(3)]
+
+    def small_step():
+        n.convolve_axes(xi, yi, taps3, BorderMode.Reflect)
+        n.convolve_axes_adjoint(wi, xi, gi, taps3, BorderMode.Reflect, T)
+
+    ms = time_call(small_step, it)
+    out["learnable_3tap_step_f32_8x192^3"] = {"ms": round(ms, 4), "gvoxel_s": round(X.numel() / ms / 1e6, 2),
+                                              "note": "forward + dL/dX + 9 tap gradients"}
+    del X, W, Y, GX, xi, wi, yi, gi
     out["dog_f32_4096^2_5scales"] = dog_form(g, it, hbm)
     # downsample (convolution.h:241-305): a {3, 15360, 8640} uint8 colour
     # image (channel axis 0, 398 MB) by 2; algorithmic bytes = source + result
