@@ -1632,6 +1632,50 @@ ndlgpu_status ndlgpu_convolve_ex(const ndlgpu_view* src, const ndlgpu_view* dst,
     else if (precision == NDLGPU_PREC_AUTO && !dtype_integral(dst->dtype) && dst->dtype != NDLGPU_F64 &&
              src->dtype != NDLGPU_F64)
         acc = Acc::F32;
+    // integral sources of up to 16 bits with a 2-D / 3-D kernel of up to 9
+    // taps per axis, exact double arithmetic: the tiled exact stencil
+    // (stencil.cu; zero taps included, which leaves integral sums unchanged)
+    if (acc == Acc::F64 && (src->dtype == NDLGPU_U8 || src->dtype == NDLGPU_U16 || src->dtype == NDLGPU_I16) &&
+        (R == 2 || R == 3)) {
+        bool fits = true;
+        for (int i = 0; i < R; i++) fits = fits && kernel->extent[i] <= kStencilMaxTaps;
+        if (fits) {
+            StencilParams sp;
+            std::memset(&sp, 0, sizeof(sp));
+            sp.srcc = static_cast<const char*>(src->data);
+            sp.dstc = static_cast<char*>(dst->data);
+            sp.sdt = src->dtype;
+            sp.ddt = dst->dtype;
+            sp.nx = (int)src->extent[0];
+            sp.ny = (int)src->extent[1];
+            sp.nz = R == 3 ? (int)src->extent[2] : 1;
+            sp.nb = 1;
+            sp.sx = src->stride[0];
+            sp.sy = src->stride[1];
+            sp.sz = R == 3 ? src->stride[2] : 0;
+            sp.dx = dst->stride[0];
+            sp.dy = dst->stride[1];
+            sp.dz = R == 3 ? dst->stride[2] : 0;
+            sp.kx = (int)kernel->extent[0];
+            sp.ky = (int)kernel->extent[1];
+            sp.kz = R == 3 ? (int)kernel->extent[2] : 1;
+            sp.cx = sp.kx / 2;
+            sp.cy = sp.ky / 2;
+            sp.cz = sp.kz / 2;
+            sp.border = border;
+            // every tap, zeros included, in coordinates() order
+            int t = 0;
+            for (int z = 0; z < sp.kz; z++)
+                for (int y = 0; y < sp.ky; y++)
+                    for (int x = 0; x < sp.kx; x++) {
+                        int64_t ko = x * kernel->stride[0] + y * kernel->stride[1];
+                        if (R == 3) ko += z * kernel->stride[2];
+                        sp.wd[t++] = host_value(kernel, ko);
+                    }
+            cudaError_t e = launch_stencil_exact(sp, (cudaStream_t)stream);
+            return e == cudaSuccess ? NDLGPU_OK : cuda_fail(e, "exact stencil launch");
+        }
+    }
     // f32 images with a dense 2-D / 3-D kernel of up to 9 taps per axis: the
     // tiled stencil (stencil.cu)
     if (acc == Acc::F32 && src->dtype == NDLGPU_F32 && dst->dtype == NDLGPU_F32 && (R == 2 || R == 3) &&

@@ -331,8 +331,11 @@ cudaError_t launch_box_blur(const BoxParams& p, cudaStream_t s);
 // Full 2-D / 3-D kernels on f32 images (stencil.cu).
 constexpr int kStencilMaxTaps = 9;
 struct StencilParams {
-    const float* src;
+    const float* src;                      // f32 path (FP32 accumulation)
     float* dst;
+    const char* srcc;                      // exact path: any <= 16-bit integral source,
+    char* dstc;                            // any destination type
+    int sdt, ddt;
     int nx, ny, nz, nb;                    // image extents (nz = 1 for images), batch count
     int64_t sx, sy, sz, sb, dx, dy, dz, db;
     int kx, ky, kz, cx, cy, cz;            // kernel extents and centres (K/2)
@@ -340,8 +343,11 @@ struct StencilParams {
     int tx, ty, tz, gx, gy;                // output box and grid (set at launch)
     int lgx, lgy;                          // log2(tx / 4), log2(ty)
     float w[kStencilMaxTaps * kStencilMaxTaps * kStencilMaxTaps];   // coordinates() order
+    double wd[kStencilMaxTaps * kStencilMaxTaps * kStencilMaxTaps];  // the same taps, exact path
 };
 cudaError_t launch_stencil(StencilParams p, cudaStream_t s);
+// The reference's own double sequence (bit-exact) for integral sources.
+cudaError_t launch_stencil_exact(StencilParams p, cudaStream_t s);
 
 // Batched form (batch.cu): one persistent launch over a table of instances.
 constexpr int kBatchMaxTaps = 37;

@@ -699,3 +699,28 @@ def test_full_kernel_f32_stencil(kshape, border):
     ref = O.convolve_total(logical, k, border)
     mag = O.convolve_total(np.abs(logical.astype(np.float64)), np.abs(k), border)
     assert_close(host(o.tensor()), ref, mag, 1e-6, "stencil %s border %d" % (kshape, border))
+
+
+@pytest.mark.parametrize("dt,odt", [(np.uint8, np.uint8), (np.int16, np.int32), (np.int16, np.float32),
+                                    (np.uint8, np.float64)])
+@pytest.mark.parametrize("kshape", [(3, 3), (5, 4), (9, 9), (3, 3, 3), (1, 5, 5), (4, 2, 3)])
+@pytest.mark.parametrize("border", [0, 1, 2])
+def test_full_kernel_integral_exact(dt, odt, kshape, border):
+    """convolve() with a full 2-D / 3-D kernel on integral sources of up to
+    16 bits: the exact tiled stencil, bit for bit with the oracle's double
+    sequence and DstT cast (truncation), zero taps and a mirrored view
+    included."""
+    rng = np.random.default_rng(sum(kshape) + 3 * border + np.dtype(dt).itemsize)
+    shape = (70, 90) if len(kshape) == 2 else (17, 26, 33)
+    lo, hi = (0, 250) if dt == np.uint8 else (-300, 300)
+    x = rng.integers(lo, hi, shape).astype(dt)
+    k = rng.standard_normal(kshape)
+    k[rng.random(kshape) < 0.15] = 0.0
+    v = Image.from_tensor(dev(x)).mirror(0)
+    logical = v.tensor().cpu().numpy()
+    o = Image.empty(v.extent(), torch.from_numpy(np.zeros(1, odt)).dtype)
+    # a float32 result accumulates in FP32 by default; EXACT asks for the
+    # reference's double sequence there too
+    n.convolve(v, o, k, border, precision=abi.PREC_EXACT if odt == np.float32 else abi.PREC_AUTO)
+    ref = O.cast(O.convolve_total(logical, k, border), O.dtype_code(np.zeros(1, odt)), O.STORE_CAST)
+    assert (host(o.tensor()) == ref).all()
