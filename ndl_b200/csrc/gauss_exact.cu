@@ -1,0 +1,94 @@
+// gauss_exact.cu -- ndl::gaussian_blur (processing/convolution.h:107-186) of
+// a 2-D integral image (sources of up to 16 bits, exact in float) in one
+// pass over it, with the reference's own double arithmetic: pass 0 along x
+// into double, pass 1 along y in double, each sum `total = total + x * w` in
+// tap order with every product and sum rounded (convolution.h:66-68, no
+// contraction), then std::round and DstT's cast (:180-185).  The reference
+// runs the two passes through two full double images; here a CTA loads its
+// 64 x 32 output box with the y and x halos once (each coordinate
+// border-mapped, mathHelpers.h:23-25), runs the x pass over the rows the y
+// pass needs into a double tile, and the y pass from it, so the results are
+// the reference's bit for bit with one read of the source and one write.
+#include "dtype.cuh"
+
+namespace ndlgpu {
+namespace {
+
+constexpr int GX = 64, GY = 32, GNT = 256;
+
+__device__ __forceinline__ int gmap(int border, int n, int x)
+{
+    const int m = map_border32(border, n, x);
+    return m < 0 ? 0 : (m >= n ? n - 1 : m);
+}
+
+template <class T>
+__global__ void __launch_bounds__(GNT) k_gauss2d_exact(const __grid_constant__ GaussExactParams p)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int SW = GX + p.kx - 1, SH = GY + p.ky - 1;
+    double* s_x = reinterpret_cast<double*>(smem);                  // SH x GX
+    float* s_src = reinterpret_cast<float*>(smem + (size_t)SH * GX * sizeof(double));   // SH x SW
+    const int x0 = blockIdx.x * GX, y0 = blockIdx.y * GY;
+    const T* src = reinterpret_cast<const T*>(p.src) + (int64_t)blockIdx.z * p.sb;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int r = warp; r < SH; r += GNT / 32) {
+        const int64_t rowoff = (int64_t)gmap(p.border, p.ny, y0 - p.cy + r) * p.sy;
+        for (int c = lane; c < SW; c += 32)
+            s_src[r * SW + c] = (float)__ldg(src + rowoff + (int64_t)gmap(p.border, p.nx, x0 - p.cx + c) * p.sx);
+    }
+    __syncthreads();
+    // x pass over every row the y pass reads
+    for (int i = threadIdx.x; i < SH * GX; i += GNT) {
+        const int r = i / GX, c = i - r * GX;
+        const float* row = s_src + r * SW + c;
+        double t = 0.0;
+        for (int k = 0; k < p.kx; k++) t = __dadd_rn(t, __dmul_rn((double)row[k], p.wx[k]));
+        s_x[i] = t;
+    }
+    __syncthreads();
+    // y pass, round, cast
+    char* dst = p.dst + (int64_t)blockIdx.z * p.db * p.des;
+    for (int i = threadIdx.x; i < GY * GX; i += GNT) {
+        const int r = i / GX, c = i - r * GX;
+        const int ox = x0 + c, oy = y0 + r;
+        if (ox >= p.nx || oy >= p.ny) continue;
+        double t = 0.0;
+        for (int k = 0; k < p.ky; k++) t = __dadd_rn(t, __dmul_rn(s_x[(r + k) * GX + c], p.wy[k]));
+        store_from(dst, p.ddt, (int64_t)ox * p.dx + (int64_t)oy * p.dy, t, p.store_mode);
+    }
+}
+
+}  // namespace
+
+size_t gauss2d_exact_smem(int kx, int ky)
+{
+    const int SW = GX + kx - 1, SH = GY + ky - 1;
+    return (size_t)SH * GX * sizeof(double) + (size_t)SH * SW * sizeof(float);
+}
+
+cudaError_t launch_gauss2d_exact(const GaussExactParams& p, cudaStream_t s)
+{
+    const size_t smem = gauss2d_exact_smem(p.kx, p.ky);
+    if (smem > 200 * 1024 || p.nb > 65535) return cudaErrorInvalidConfiguration;
+    static size_t configured = 0;
+    if (smem > configured) {
+        for (auto f : {k_gauss2d_exact<uint8_t>, k_gauss2d_exact<uint16_t>, k_gauss2d_exact<int16_t>}) {
+            cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+        }
+        configured = smem;
+    }
+    const dim3 grid((unsigned)((p.nx + GX - 1) / GX), (unsigned)((p.ny + GY - 1) / GY), (unsigned)p.nb);
+    if (grid.y > 65535) return cudaErrorInvalidConfiguration;
+    switch (p.sdt) {
+    case NDLGPU_U8: k_gauss2d_exact<uint8_t><<<grid, GNT, smem, s>>>(p); break;
+    case NDLGPU_U16: k_gauss2d_exact<uint16_t><<<grid, GNT, smem, s>>>(p); break;
+    case NDLGPU_I16: k_gauss2d_exact<int16_t><<<grid, GNT, smem, s>>>(p); break;
+    default: return cudaErrorInvalidValue;
+    }
+    count_launch();
+    return cudaGetLastError();
+}
+
+}  // namespace ndlgpu

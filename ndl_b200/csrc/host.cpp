@@ -1537,6 +1537,45 @@ ndlgpu_status ndlgpu_gaussian_blur_workspace_size(const ndlgpu_view* src, const 
     return NDLGPU_OK;
 }
 
+// 2-D integral images (at most 16 bits) blurred into an integral or f64
+// image: the reference's double arithmetic in one fused kernel
+// (gauss_exact.cu).  False when not eligible.
+static bool gauss2d_exact(const ndlgpu_view* src, const ndlgpu_view* dst, const std::vector<LPass>& lp, int border,
+                          cudaStream_t s, cudaError_t* err)
+{
+    if (src->rank != 2 || lp.size() != 2) return false;
+    if (src->dtype != NDLGPU_U8 && src->dtype != NDLGPU_U16 && src->dtype != NDLGPU_I16) return false;
+    if (!(dtype_integral(dst->dtype) || dst->dtype == NDLGPU_F64)) return false;
+    if (lp[0].axis != 0 || lp[1].axis != 1) return false;
+    const int kx = (int)lp[0].taps.size(), ky = (int)lp[1].taps.size();
+    if (kx > 61 || ky > 61) return false;
+    if (src->extent[0] > 0x7fffffffLL || src->extent[1] > 0x7fffffffLL) return false;
+    GaussExactParams p;
+    std::memset(&p, 0, sizeof(p));
+    p.src = static_cast<const char*>(src->data);
+    p.dst = static_cast<char*>(dst->data);
+    p.sdt = src->dtype;
+    p.ddt = dst->dtype;
+    p.des = dtype_size(dst->dtype);
+    p.nx = (int)src->extent[0];
+    p.ny = (int)src->extent[1];
+    p.nb = 1;
+    p.sx = src->stride[0];
+    p.sy = src->stride[1];
+    p.dx = dst->stride[0];
+    p.dy = dst->stride[1];
+    p.kx = kx;
+    p.ky = ky;
+    p.cx = lp[0].center;
+    p.cy = lp[1].center;
+    p.border = border;
+    p.store_mode = STORE_ROUND;
+    for (int k = 0; k < kx; k++) p.wx[k] = lp[0].taps[k];
+    for (int k = 0; k < ky; k++) p.wy[k] = lp[1].taps[k];
+    *err = launch_gauss2d_exact(p, s);
+    return true;
+}
+
 ndlgpu_status ndlgpu_gaussian_blur(const ndlgpu_view* src, const ndlgpu_view* dst, double sigma, int border,
                                    void* workspace, size_t workspace_bytes, void* stream)
 {
@@ -1548,6 +1587,9 @@ ndlgpu_status ndlgpu_gaussian_blur(const ndlgpu_view* src, const ndlgpu_view* ds
     Plan pl;
     st = prepare(src, dst, lp, border, NDLGPU_ROUND_ONCE, NDLGPU_PREC_AUTO, &c, &pl);
     if (st != NDLGPU_OK || c.total == 0) return st;
+    cudaError_t e = cudaSuccess;
+    if (gauss2d_exact(src, dst, lp, border, (cudaStream_t)stream, &e))
+        return e == cudaSuccess ? NDLGPU_OK : cuda_fail(e, "exact 2-D gaussian");
     return execute(c, pl, NDLGPU_ROUND_ONCE, border, workspace, workspace_bytes, (cudaStream_t)stream);
 }
 

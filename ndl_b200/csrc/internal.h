@@ -328,6 +328,22 @@ struct BoxParams {
 };
 cudaError_t launch_box_blur(const BoxParams& p, cudaStream_t s);
 
+// gaussian_blur of 2-D integral images in the reference's double arithmetic
+// (gauss_exact.cu).
+struct GaussExactParams {
+    const char* src;
+    char* dst;
+    int sdt, ddt, des;                     // des: destination element bytes
+    int nx, ny, nb;                        // image extents, batch count
+    int64_t sx, sy, sb, dx, dy, db;
+    int kx, ky, cx, cy;
+    int border;
+    int store_mode;                        // STORE_ROUND (two passes) or STORE_CAST
+    double wx[128], wy[128];
+};
+size_t gauss2d_exact_smem(int kx, int ky);
+cudaError_t launch_gauss2d_exact(const GaussExactParams& p, cudaStream_t s);
+
 // Full 2-D / 3-D kernels on f32 images (stencil.cu).
 constexpr int kStencilMaxTaps = 9;
 struct StencilParams {
