@@ -1605,6 +1605,9 @@ ndlgpu_status ndlgpu_gaussian_blur_axes(const ndlgpu_view* src, const ndlgpu_vie
     Plan pl;
     st = prepare(src, dst, lp, border, NDLGPU_ROUND_ONCE, NDLGPU_PREC_AUTO, &c, &pl);
     if (st != NDLGPU_OK || c.total == 0) return st;
+    cudaError_t e = cudaSuccess;
+    if (gauss2d_exact(src, dst, lp, border, (cudaStream_t)stream, &e))
+        return e == cudaSuccess ? NDLGPU_OK : cuda_fail(e, "exact 2-D gaussian");
     return execute(c, pl, NDLGPU_ROUND_ONCE, border, workspace, workspace_bytes, (cudaStream_t)stream);
 }
 

@@ -742,3 +742,17 @@ def test_gaussian_blur_integral_image_exact(dt, odt, sigma, border):
     n.gaussian_blur(v, o, sigma, border)
     ref = O.gaussian_blur(logical, sigma, border, O.dtype_code(np.zeros(1, odt)))
     assert (host(o.tensor()) == ref).all()
+
+
+@pytest.mark.parametrize("border", [0, 1, 2])
+def test_gaussian_blur_axes_integral_image_exact(border):
+    """gaussian_blur_axes with a different sigma per axis on a 2-D uint8
+    image: the fused exact kernel, bit for bit with the oracle's gaussian
+    structure (one final round)."""
+    rng = np.random.default_rng(40 + border)
+    x = rng.integers(0, 256, (97, 131)).astype(np.uint8)
+    s = Image.from_tensor(dev(x))
+    o = Image.empty(s.extent(), torch.uint8)
+    n.gaussian_blur_axes(s, o, [1.3, 2.7], border)
+    ref = O.compose(x, [(0, O.gaussian_weights(1.3)), (1, O.gaussian_weights(2.7))], border, O.U8, O.STORE_ROUND)
+    assert (host(o.tensor()) == ref).all()
