@@ -1540,6 +1540,9 @@ ndlgpu_status ndlgpu_gaussian_blur_workspace_size(const ndlgpu_view* src, const 
 // 2-D integral images (at most 16 bits) blurred into an integral or f64
 // image: the reference's double arithmetic in one fused kernel
 // (gauss_exact.cu).  False when not eligible.
+static ndlgpu_status gauss3d_exact(const ndlgpu_view* src, const ndlgpu_view* dst, const std::vector<LPass>& lp,
+                                   int border, void* ws, size_t ws_bytes, cudaStream_t s, bool* done);
+
 static bool gauss2d_exact(const ndlgpu_view* src, const ndlgpu_view* dst, const std::vector<LPass>& lp, int border,
                           cudaStream_t s, cudaError_t* err)
 {
@@ -1576,6 +1579,75 @@ static bool gauss2d_exact(const ndlgpu_view* src, const ndlgpu_view* dst, const 
     return true;
 }
 
+// 3-D integral volumes (at most 16 bits) blurred into an integral or f64
+// volume: every z plane through the fused exact x/y kernel into a double
+// image (bufB of the reference's gaussian_blur), then the z pass in the
+// same double arithmetic with the one final round.  *done = false when not
+// eligible.
+static ndlgpu_status gauss3d_exact(const ndlgpu_view* src, const ndlgpu_view* dst, const std::vector<LPass>& lp,
+                                   int border, void* ws, size_t ws_bytes, cudaStream_t s, bool* done)
+{
+    *done = false;
+    if (src->rank != 3 || lp.size() != 3) return NDLGPU_OK;
+    if (src->dtype != NDLGPU_U8 && src->dtype != NDLGPU_U16 && src->dtype != NDLGPU_I16) return NDLGPU_OK;
+    if (!(dtype_integral(dst->dtype) || dst->dtype == NDLGPU_F64)) return NDLGPU_OK;
+    if (lp[0].axis != 0 || lp[1].axis != 1 || lp[2].axis != 2) return NDLGPU_OK;
+    const int kx = (int)lp[0].taps.size(), ky = (int)lp[1].taps.size();
+    if (kx > 61 || ky > 61 || src->extent[2] > 65535) return NDLGPU_OK;
+    const int64_t count = view_count(src);
+    if (count >= (int64_t(1) << 31)) return NDLGPU_OK;
+    Scratch sc;
+    ndlgpu_status st = get_scratch(align_up((size_t)count * sizeof(double)), ws, ws_bytes, s, &sc);
+    if (st != NDLGPU_OK) return st;
+    const int64_t nx = src->extent[0], ny = src->extent[1];
+    GaussExactParams p;
+    std::memset(&p, 0, sizeof(p));
+    p.src = static_cast<const char*>(src->data);
+    p.dst = static_cast<char*>(sc.base);
+    p.sdt = src->dtype;
+    p.ddt = NDLGPU_F64;
+    p.des = 8;
+    p.nx = (int)nx;
+    p.ny = (int)ny;
+    p.nb = (int)src->extent[2];
+    p.sx = src->stride[0];
+    p.sy = src->stride[1];
+    p.sb = src->stride[2];
+    p.dx = 1;
+    p.dy = nx;
+    p.db = nx * ny;
+    p.kx = kx;
+    p.ky = ky;
+    p.cx = lp[0].center;
+    p.cy = lp[1].center;
+    p.border = border;
+    p.store_mode = STORE_CAST;         // double intermediate: no rounding
+    for (int k = 0; k < kx; k++) p.wx[k] = lp[0].taps[k];
+    for (int k = 0; k < ky; k++) p.wy[k] = lp[1].taps[k];
+    cudaError_t e = launch_gauss2d_exact(p, s);
+    if (e != cudaSuccess) return cuda_fail(e, "exact x/y gaussian");
+    // the z pass: the general exact pass over the double image
+    Canon geo;
+    geo.total = count;
+    for (int i = 0; i < 3; i++) geo.ax.push_back(CAxis{src->extent[i], 0, 0, i});
+    CPass zp;
+    zp.axis = 2;
+    for (size_t k = 0; k < lp[2].taps.size(); k++)
+        if (lp[2].taps[k] != 0.0) {
+            zp.off.push_back((int)k - lp[2].center);
+            zp.w.push_back(lp[2].taps[k]);
+        }
+    const std::vector<int64_t> cst = contiguous_strides(geo);
+    std::vector<int64_t> dst_st(3);
+    for (int i = 0; i < 3; i++) dst_st[i] = dst->stride[i];
+    const std::vector<int32_t> none;
+    st = run_generic_pass(Acc::F64, geo, zp, static_cast<const char*>(sc.base), NDLGPU_F64, cst,
+                          static_cast<char*>(dst->data), dst->dtype, dst_st, border, STORE_ROUND, 0, none, s);
+    if (st != NDLGPU_OK) return st;
+    *done = true;
+    return NDLGPU_OK;
+}
+
 ndlgpu_status ndlgpu_gaussian_blur(const ndlgpu_view* src, const ndlgpu_view* dst, double sigma, int border,
                                    void* workspace, size_t workspace_bytes, void* stream)
 {
@@ -1590,6 +1662,9 @@ ndlgpu_status ndlgpu_gaussian_blur(const ndlgpu_view* src, const ndlgpu_view* ds
     cudaError_t e = cudaSuccess;
     if (gauss2d_exact(src, dst, lp, border, (cudaStream_t)stream, &e))
         return e == cudaSuccess ? NDLGPU_OK : cuda_fail(e, "exact 2-D gaussian");
+    bool done = false;
+    st = gauss3d_exact(src, dst, lp, border, workspace, workspace_bytes, (cudaStream_t)stream, &done);
+    if (st != NDLGPU_OK || done) return st;
     return execute(c, pl, NDLGPU_ROUND_ONCE, border, workspace, workspace_bytes, (cudaStream_t)stream);
 }
 
@@ -1608,6 +1683,9 @@ ndlgpu_status ndlgpu_gaussian_blur_axes(const ndlgpu_view* src, const ndlgpu_vie
     cudaError_t e = cudaSuccess;
     if (gauss2d_exact(src, dst, lp, border, (cudaStream_t)stream, &e))
         return e == cudaSuccess ? NDLGPU_OK : cuda_fail(e, "exact 2-D gaussian");
+    bool done = false;
+    st = gauss3d_exact(src, dst, lp, border, workspace, workspace_bytes, (cudaStream_t)stream, &done);
+    if (st != NDLGPU_OK || done) return st;
     return execute(c, pl, NDLGPU_ROUND_ONCE, border, workspace, workspace_bytes, (cudaStream_t)stream);
 }
 
