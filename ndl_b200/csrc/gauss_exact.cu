@@ -38,24 +38,51 @@ __global__ void __launch_bounds__(GNT) k_gauss2d_exact(const __grid_constant__ G
             s_src[r * SW + c] = (float)__ldg(src + rowoff + (int64_t)gmap(p.border, p.nx, x0 - p.cx + c) * p.sx);
     }
     __syncthreads();
-    // x pass over every row the y pass reads
-    for (int i = threadIdx.x; i < SH * GX; i += GNT) {
-        const int r = i / GX, c = i - r * GX;
+    // x pass over every row the y pass reads; units of 4 consecutive
+    // outputs, whose 4 sums are independent chains (the sum of one output
+    // is a chain of dependent double additions)
+    for (int i = threadIdx.x; i < SH * (GX / 4); i += GNT) {
+        const int r = i / (GX / 4), c = 4 * (i - r * (GX / 4));
         const float* row = s_src + r * SW + c;
-        double t = 0.0;
-        for (int k = 0; k < p.kx; k++) t = __dadd_rn(t, __dmul_rn((double)row[k], p.wx[k]));
-        s_x[i] = t;
+        double t[4] = {0.0, 0.0, 0.0, 0.0};
+        float v0 = row[0], v1 = row[1], v2 = row[2];
+        for (int k = 0; k < p.kx; k++) {
+            const float v3 = row[k + 3];     // column c + kx + 2 < SW at most
+            const double wk = p.wx[k];
+            t[0] = __dadd_rn(t[0], __dmul_rn((double)v0, wk));
+            t[1] = __dadd_rn(t[1], __dmul_rn((double)v1, wk));
+            t[2] = __dadd_rn(t[2], __dmul_rn((double)v2, wk));
+            t[3] = __dadd_rn(t[3], __dmul_rn((double)v3, wk));
+            v0 = v1;
+            v1 = v2;
+            v2 = v3;
+        }
+        double* xo = s_x + r * GX + c;
+        xo[0] = t[0];
+        xo[1] = t[1];
+        xo[2] = t[2];
+        xo[3] = t[3];
     }
     __syncthreads();
-    // y pass, round, cast
+    // y pass, round, cast: each thread sums 4 outputs of a row GX/4 apart,
+    // so that a warp's shared-memory reads are consecutive doubles
     char* dst = p.dst + (int64_t)blockIdx.z * p.db * p.des;
-    for (int i = threadIdx.x; i < GY * GX; i += GNT) {
-        const int r = i / GX, c = i - r * GX;
-        const int ox = x0 + c, oy = y0 + r;
-        if (ox >= p.nx || oy >= p.ny) continue;
-        double t = 0.0;
-        for (int k = 0; k < p.ky; k++) t = __dadd_rn(t, __dmul_rn(s_x[(r + k) * GX + c], p.wy[k]));
-        store_from(dst, p.ddt, (int64_t)ox * p.dx + (int64_t)oy * p.dy, t, p.store_mode);
+    for (int i = threadIdx.x; i < GY * (GX / 4); i += GNT) {
+        const int r = i / (GX / 4), c = i - r * (GX / 4);
+        const int oy = y0 + r;
+        if (oy >= p.ny) continue;
+        double t[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int k = 0; k < p.ky; k++) {
+            const double* xr = s_x + (r + k) * GX + c;
+            const double wk = p.wy[k];
+#pragma unroll
+            for (int m = 0; m < 4; m++) t[m] = __dadd_rn(t[m], __dmul_rn(xr[m * (GX / 4)], wk));
+        }
+#pragma unroll
+        for (int m = 0; m < 4; m++) {
+            const int ox = x0 + c + m * (GX / 4);
+            if (ox < p.nx) store_from(dst, p.ddt, (int64_t)ox * p.dx + (int64_t)oy * p.dy, t[m], p.store_mode);
+        }
     }
 }
 
