@@ -86,6 +86,41 @@ __global__ void __launch_bounds__(GNT) k_gauss2d_exact(const __grid_constant__ G
     }
 }
 
+// The z pass of a 3-D integral gaussian over the double volume the x/y
+// kernel wrote (the reference's bufB): each thread owns one (x, y) column
+// and ZC consecutive outputs along z, ZC independent chains over a sliding
+// register window of the column (border-mapped per plane), then the final
+// round and DstT's cast.  Consecutive threads read consecutive x of a
+// plane; the planes a chunk shares with its neighbours stay in L2.
+constexpr int ZC = 8, ZNT = 256;
+
+__global__ void __launch_bounds__(ZNT) k_gauss_z_exact(const __grid_constant__ GaussZExactParams p)
+{
+    const int64_t plane = (int64_t)p.nx * p.ny;
+    const int64_t xy = (int64_t)blockIdx.x * ZNT + threadIdx.x;
+    if (xy >= plane) return;
+    const int z0 = blockIdx.y * ZC;
+    const double* col = p.src + xy;
+    double t[ZC], v[ZC];
+#pragma unroll
+    for (int m = 0; m < ZC; m++) t[m] = 0.0;
+#pragma unroll
+    for (int m = 0; m < ZC - 1; m++) v[m] = col[plane * gmap(p.border, p.nz, z0 - p.cz + m)];
+    for (int k = 0; k < p.kz; k++) {
+        v[ZC - 1] = col[plane * gmap(p.border, p.nz, z0 - p.cz + k + ZC - 1)];
+        const double wk = p.wz[k];
+#pragma unroll
+        for (int m = 0; m < ZC; m++) t[m] = __dadd_rn(t[m], __dmul_rn(v[m], wk));
+#pragma unroll
+        for (int m = 0; m < ZC - 1; m++) v[m] = v[m + 1];
+    }
+    const int x = (int)(xy % p.nx), y = (int)(xy / p.nx);
+    const int64_t o = (int64_t)x * p.dx + (int64_t)y * p.dy;
+#pragma unroll
+    for (int m = 0; m < ZC; m++)
+        if (z0 + m < p.nz) store_from(p.dst, p.ddt, o + (int64_t)(z0 + m) * p.dz, t[m], STORE_ROUND);
+}
+
 }  // namespace
 
 size_t gauss2d_exact_smem(int kx, int ky)
@@ -114,6 +149,16 @@ cudaError_t launch_gauss2d_exact(const GaussExactParams& p, cudaStream_t s)
     case NDLGPU_I16: k_gauss2d_exact<int16_t><<<grid, GNT, smem, s>>>(p); break;
     default: return cudaErrorInvalidValue;
     }
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gauss_z_exact(const GaussZExactParams& p, cudaStream_t s)
+{
+    const int64_t plane = (int64_t)p.nx * p.ny;
+    const int64_t gx = (plane + ZNT - 1) / ZNT, gy = (p.nz + ZC - 1) / ZC;
+    if (gx > 0x7fffffff || gy > 65535 || p.kz > 128) return cudaErrorInvalidConfiguration;
+    k_gauss_z_exact<<<dim3((unsigned)gx, (unsigned)gy), ZNT, 0, s>>>(p);
     count_launch();
     return cudaGetLastError();
 }

@@ -1593,7 +1593,7 @@ static ndlgpu_status gauss3d_exact(const ndlgpu_view* src, const ndlgpu_view* ds
     if (!(dtype_integral(dst->dtype) || dst->dtype == NDLGPU_F64)) return NDLGPU_OK;
     if (lp[0].axis != 0 || lp[1].axis != 1 || lp[2].axis != 2) return NDLGPU_OK;
     const int kx = (int)lp[0].taps.size(), ky = (int)lp[1].taps.size();
-    if (kx > 61 || ky > 61 || src->extent[2] > 65535) return NDLGPU_OK;
+    if (kx > 61 || ky > 61 || lp[2].taps.size() > 128 || src->extent[2] > 65535) return NDLGPU_OK;
     const int64_t count = view_count(src);
     if (count >= (int64_t(1) << 31)) return NDLGPU_OK;
     Scratch sc;
@@ -1626,24 +1626,24 @@ static ndlgpu_status gauss3d_exact(const ndlgpu_view* src, const ndlgpu_view* ds
     for (int k = 0; k < ky; k++) p.wy[k] = lp[1].taps[k];
     cudaError_t e = launch_gauss2d_exact(p, s);
     if (e != cudaSuccess) return cuda_fail(e, "exact x/y gaussian");
-    // the z pass: the general exact pass over the double image
-    Canon geo;
-    geo.total = count;
-    for (int i = 0; i < 3; i++) geo.ax.push_back(CAxis{src->extent[i], 0, 0, i});
-    CPass zp;
-    zp.axis = 2;
-    for (size_t k = 0; k < lp[2].taps.size(); k++)
-        if (lp[2].taps[k] != 0.0) {
-            zp.off.push_back((int)k - lp[2].center);
-            zp.w.push_back(lp[2].taps[k]);
-        }
-    const std::vector<int64_t> cst = contiguous_strides(geo);
-    std::vector<int64_t> dst_st(3);
-    for (int i = 0; i < 3; i++) dst_st[i] = dst->stride[i];
-    const std::vector<int32_t> none;
-    st = run_generic_pass(Acc::F64, geo, zp, static_cast<const char*>(sc.base), NDLGPU_F64, cst,
-                          static_cast<char*>(dst->data), dst->dtype, dst_st, border, STORE_ROUND, 0, none, s);
-    if (st != NDLGPU_OK) return st;
+    // the z pass over the double volume, rounded and cast
+    GaussZExactParams z;
+    std::memset(&z, 0, sizeof(z));
+    z.src = static_cast<const double*>(sc.base);
+    z.dst = static_cast<char*>(dst->data);
+    z.ddt = dst->dtype;
+    z.nx = (int)nx;
+    z.ny = (int)ny;
+    z.nz = (int)src->extent[2];
+    z.dx = dst->stride[0];
+    z.dy = dst->stride[1];
+    z.dz = dst->stride[2];
+    z.kz = (int)lp[2].taps.size();
+    z.cz = lp[2].center;
+    z.border = border;
+    for (int k = 0; k < z.kz; k++) z.wz[k] = lp[2].taps[k];
+    e = launch_gauss_z_exact(z, s);
+    if (e != cudaSuccess) return cuda_fail(e, "exact z gaussian");
     *done = true;
     return NDLGPU_OK;
 }

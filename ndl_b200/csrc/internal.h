@@ -343,6 +343,19 @@ struct GaussExactParams {
 };
 size_t gauss2d_exact_smem(int kx, int ky);
 cudaError_t launch_gauss2d_exact(const GaussExactParams& p, cudaStream_t s);
+// The exact z pass of a 3-D integral gaussian over a contiguous double
+// volume (x fastest), rounded and cast into dst.
+struct GaussZExactParams {
+    const double* src;
+    char* dst;
+    int ddt;
+    int nx, ny, nz;
+    int64_t dx, dy, dz;
+    int kz, cz;
+    int border;
+    double wz[128];
+};
+cudaError_t launch_gauss_z_exact(const GaussZExactParams& p, cudaStream_t s);
 
 // Full 2-D / 3-D kernels on f32 images (stencil.cu).
 constexpr int kStencilMaxTaps = 9;

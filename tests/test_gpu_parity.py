@@ -774,3 +774,19 @@ def test_gaussian_blur_integral_volume_exact(dt, odt, sigma, border):
     n.gaussian_blur(v, o, sigma, border)
     ref = O.gaussian_blur(logical, sigma, border, O.dtype_code(np.zeros(1, odt)))
     assert (host(o.tensor()) == ref).all()
+
+
+@pytest.mark.parametrize("border", [0, 1, 2])
+def test_gaussian_blur_integral_volume_exact_strided_dst(border):
+    """The exact z pass stores through a mirrored, padded destination view;
+    z extents that are not a multiple of the kernel's z chunk."""
+    rng = np.random.default_rng(31 + border)
+    x = rng.integers(0, 256, (13, 30, 37)).astype(np.uint8)
+    v = Image.from_tensor(dev(x))
+    buf = torch.zeros((13, 30, 40), dtype=torch.uint8, device="cuda")
+    ext = v.extent()
+    o = Image.from_tensor(buf).view((0, 0, 0), (ext[0] - 1, ext[1] - 1, ext[2] - 1)).mirror(2).mirror(0)
+    assert o.extent() == ext
+    n.gaussian_blur(v, o, 1.7, border)
+    ref = O.gaussian_blur(x, 1.7, border, O.U8)
+    assert (host(o.tensor()) == ref).all()
