@@ -311,6 +311,17 @@ NDLGPU_API uint64_t ndlgpu_kernel_launches(void);
  * bits are reserved. */
 NDLGPU_API ndlgpu_status ndlgpu_device_status(void* stream, int32_t* code);
 
+/* Test control of the bounded device waits on the current device; no
+ * reference counterpart.  spin_limit > 0 bounds every tensor-map plane wait
+ * and batched phase wait to that many polls; unreachable != 0 makes each of
+ * those waits ask for more than ever arrives (plane loads announce 16 bytes
+ * they never deliver, phase waits one predecessor item too many), so that
+ * they run out: the kernel then sets its guard bit, lets its own copies in
+ * flight land (bounded) and returns, and ndlgpu_device_status reports it.
+ * Nothing faults.  ndlgpu_test_wait_timeouts(0, 0) restores normal
+ * operation. */
+NDLGPU_API ndlgpu_status ndlgpu_test_wait_timeouts(int spin_limit, int unreachable);
+
 #ifdef __cplusplus
 }
 #endif

@@ -101,6 +101,7 @@ SIGNATURES = {
     "ndlgpu_convolve_axes_adjoint": (_I, [_PV, _PV, _PV, _I, _PK, _I, _VP, _I, _VP, _SZ, _VP]),
     "ndlgpu_convolve_axes_adjoint_workspace_size": (_I, [_PV, _PV, _PV, _I, _PK, _I, _I, ctypes.POINTER(_SZ)]),
     "ndlgpu_device_status": (_I, [_VP, ctypes.POINTER(ctypes.c_int32)]),
+    "ndlgpu_test_wait_timeouts": (_I, [_I, _I]),
     "ndlgpu_kernel_launches": (ctypes.c_uint64, []),
     "ndlgpu_gaussian_blur_noalloc": (_I, [_PV, _PV, ctypes.c_double, _I, _VP]),
     "ndlgpu_batch_create": (_I, [ctypes.POINTER(_VP)]),

@@ -43,6 +43,10 @@ __device__ int32_t g_guard_batch;   // bit 2: a phase wait ran past its bound
 constexpr int kSeg = 128;        // row-pass outputs per warp segment
 constexpr int kColS = 64;        // column-pass outputs per unit along the axis
 constexpr int kMaxSpins = 1 << 22;
+// Test controls (ndlgpu_test_wait_timeouts): the bound of a phase wait, and
+// extra predecessor items a wait asks for that never arrive.
+__device__ int g_batch_wait_spins = kMaxSpins;
+__device__ int g_batch_need_bias = 0;
 
 template <class T> __device__ __forceinline__ float to_f(T v);
 template <> __device__ __forceinline__ float to_f<float>(float v) { return v; }
@@ -425,11 +429,12 @@ __global__ void __launch_bounds__(256, 3) k_batch(const BatchDesc* __restrict__ 
             s_skip = 0;
             if (phase > 0) {
                 volatile int* dn = done + 3 * item.x + phase - 1;
-                const int need = descs[item.x].nitems[phase - 1];
+                const int need = descs[item.x].nitems[phase - 1] + g_batch_need_bias;
+                const int max_spins = g_batch_wait_spins;
                 int spins = 0;
                 while (*dn < need) {
                     __nanosleep(200);
-                    if (++spins > kMaxSpins) {
+                    if (++spins > max_spins) {
                         atomicExch(err, 1);
                         atomicOr(&g_guard_batch, 4);
                         s_skip = 1;
@@ -560,6 +565,13 @@ cudaError_t batch_prepare(int dtype, int cfg, BatchLaunch* L)
     case NDLGPU_F16: return prepare_b<__half>(w, L);
     default: return cudaErrorInvalidValue;
     }
+}
+
+cudaError_t set_batch_wait_test(int spins, int need_bias)
+{
+    cudaError_t e = cudaMemcpyToSymbol(g_batch_wait_spins, &spins, sizeof(int));
+    if (e != cudaSuccess) return e;
+    return cudaMemcpyToSymbol(g_batch_need_bias, &need_bias, sizeof(int));
 }
 
 cudaError_t read_guard_batch(int32_t* v)

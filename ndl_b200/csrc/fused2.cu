@@ -108,6 +108,11 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 __device__ int32_t g_guard_fused;
 
 constexpr int kTmaSpins = 1 << 22;   // bound on the mbarrier polls for one plane
+// Test controls (ndlgpu_test_wait_timeouts): the poll bound of a plane wait,
+// and extra bytes every plane load announces to its mbarrier but never
+// delivers, so that the wait runs out without anything faulting.
+__device__ int g_tma_wait_spins = kTmaSpins;
+__device__ unsigned g_tma_tx_bias = 0;
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count)
@@ -128,6 +133,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity)
         : "r"(smem_u32(bar)), "r"(parity)
         : "memory");
     return ok != 0;
+}
+__device__ __forceinline__ void mbar_complete_tx(uint64_t* bar, unsigned bytes)
+{
+    asm volatile("mbarrier.complete_tx.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
 // orders this thread's earlier generic-proxy shared-memory accesses before
 // the copy engine's writes that it issues next
@@ -267,6 +276,12 @@ __global__ void __launch_bounds__(8 * TY, (Occ<TY, ADJ, KZ>::value))
     // registers); every other element goes to a shared table of (shared
     // offset, in-plane global offset) pairs with its column border-mapped.
     const bool zp = ADJ && p.zero_pad;   // adjoint, Clamp/Reflect: zero outside the image
+    unsigned tx_bias = 0;
+    int wait_spins = kTmaSpins;
+    if constexpr (TMA) {
+        tx_bias = g_tma_tx_bias;
+        wait_spins = g_tma_wait_spins;
+    }
     if (tid == 0) {
         *s_ntab = 0;
         if constexpr (TMA) {
@@ -324,7 +339,7 @@ __global__ void __launch_bounds__(8 * TY, (Occ<TY, ADJ, KZ>::value))
                 const int yc = y0 - G::CY;
                 auto coord = [&](int d) { return p.tma_pos[0] == d ? yc : (p.tma_pos[1] == d ? zi : bat); };
                 fence_proxy_async();
-                mbar_expect_tx(&s_bar[stage], (unsigned)G::STAGE_BYTES);
+                mbar_expect_tx(&s_bar[stage], (unsigned)G::STAGE_BYTES + tx_bias);
                 tma_load_4d(sb, &tmap, &s_bar[stage], gx0, coord(0), coord(1), coord(2));
             }
             return;
@@ -389,10 +404,24 @@ __global__ void __launch_bounds__(8 * TY, (Occ<TY, ADJ, KZ>::value))
     for (int n = 0; n < nplanes; n++) {
         if constexpr (TMA) {
             bool ok = false;
-            for (int i = 0; i < kTmaSpins && !ok; i++) ok = mbar_try_wait(&s_bar[stage], phase);
+            for (int i = 0; i < wait_spins && !ok; i++) ok = mbar_try_wait(&s_bar[stage], phase);
             // plane n visible; every thread is past the X pass of plane n-1
             if (__syncthreads_or(!ok)) {
-                if (tid == 0) atomicOr(&g_guard_fused, 2);
+                if (tid == 0) {
+                    atomicOr(&g_guard_fused, 2);
+                    // planes n .. n+STAGES-2 may still be landing in this
+                    // CTA's ring: retire the announced surplus (test control)
+                    // and wait, bounded, for each before the CTA lets go of
+                    // its shared memory.  Plane m sits in stage m % STAGES
+                    // with parity (m / STAGES) & 1.
+                    for (int m = n; m < min(n + STAGES - 1, nplanes); m++) {
+                        uint64_t* bar = &s_bar[m % STAGES];
+                        if (tx_bias) mbar_complete_tx(bar, tx_bias);
+                        const unsigned par = (unsigned)(m / STAGES) & 1u;
+                        for (int i = 0; i < kTmaSpins && !mbar_try_wait(bar, par); i++) {
+                        }
+                    }
+                }
                 return;
             }
             if (stage + 1 == STAGES) phase ^= 1u;
@@ -746,6 +775,13 @@ bool fused2_supported(int sdt, int ddt, int kx, int ky, int kz, int adj)
     for (const Variant2& v : kVariants2)
         if (v.adj == adj && v.sdt == sdt && v.ddt == ddt && v.kx == kx && v.ky == ky && v.kz == kz) return true;
     return false;
+}
+
+cudaError_t set_tma_wait_test(int spins, unsigned tx_bias)
+{
+    cudaError_t e = cudaMemcpyToSymbol(g_tma_wait_spins, &spins, sizeof(int));
+    if (e != cudaSuccess) return e;
+    return cudaMemcpyToSymbol(g_tma_tx_bias, &tx_bias, sizeof(unsigned));
 }
 
 cudaError_t read_guard_fused(int32_t* v)

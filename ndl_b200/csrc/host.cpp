@@ -1520,6 +1520,38 @@ ndlgpu_status ndlgpu_convolve_axes(const ndlgpu_view* src, const ndlgpu_view* ds
     return execute(c, pl, compose, border, workspace, workspace_bytes, (cudaStream_t)stream);
 }
 
+// The route a gaussian_blur takes; the workspace query and the call both
+// ask this, so that the scratch reported is the scratch used.
+enum class GaussRoute { Planned, Exact2D, Exact3D };
+
+static GaussRoute gauss_route(const ndlgpu_view* src, const ndlgpu_view* dst, const std::vector<LPass>& lp,
+                              const Plan& pl)
+{
+    // an integer-numerator fused plan is already bit-exact and needs no scratch
+    if (pl.fused && pl.acc == Acc::I32) return GaussRoute::Planned;
+    const bool isrc = src->dtype == NDLGPU_U8 || src->dtype == NDLGPU_U16 || src->dtype == NDLGPU_I16;
+    if (!isrc || !(dtype_integral(dst->dtype) || dst->dtype == NDLGPU_F64)) return GaussRoute::Planned;
+    if (src->rank != (int)lp.size() || (lp.size() != 2 && lp.size() != 3)) return GaussRoute::Planned;
+    for (size_t i = 0; i < lp.size(); i++)
+        if (lp[i].axis != (int)i) return GaussRoute::Planned;
+    if (lp[0].taps.size() > 61 || lp[1].taps.size() > 61) return GaussRoute::Planned;
+    if (src->extent[0] > 0x7fffffffLL || src->extent[1] > 0x7fffffffLL) return GaussRoute::Planned;
+    if (lp.size() == 2) return GaussRoute::Exact2D;
+    if (lp[2].taps.size() > 128 || src->extent[2] > 65535) return GaussRoute::Planned;
+    if (view_count(src) >= (int64_t(1) << 31)) return GaussRoute::Planned;
+    return GaussRoute::Exact3D;
+}
+
+static size_t gauss_workspace(const ndlgpu_view* src, const ndlgpu_view* dst, const std::vector<LPass>& lp,
+                              const Canon& c, const Plan& pl)
+{
+    switch (gauss_route(src, dst, lp, pl)) {
+    case GaussRoute::Exact2D: return 0;
+    case GaussRoute::Exact3D: return align_up((size_t)view_count(src) * sizeof(double));
+    default: return plan_workspace(c, pl);
+    }
+}
+
 ndlgpu_status ndlgpu_gaussian_blur_workspace_size(const ndlgpu_view* src, const ndlgpu_view* dst, double sigma,
                                                   int border, size_t* bytes)
 {
@@ -1533,7 +1565,7 @@ ndlgpu_status ndlgpu_gaussian_blur_workspace_size(const ndlgpu_view* src, const 
     Plan pl;
     st = prepare(src, dst, lp, border, NDLGPU_ROUND_ONCE, NDLGPU_PREC_AUTO, &c, &pl);
     if (st != NDLGPU_OK || c.total == 0) return st;
-    *bytes = plan_workspace(c, pl);
+    *bytes = gauss_workspace(src, dst, lp, c, pl);
     return NDLGPU_OK;
 }
 
@@ -1659,11 +1691,13 @@ ndlgpu_status ndlgpu_gaussian_blur(const ndlgpu_view* src, const ndlgpu_view* ds
     Plan pl;
     st = prepare(src, dst, lp, border, NDLGPU_ROUND_ONCE, NDLGPU_PREC_AUTO, &c, &pl);
     if (st != NDLGPU_OK || c.total == 0) return st;
+    const GaussRoute route = gauss_route(src, dst, lp, pl);
     cudaError_t e = cudaSuccess;
-    if (gauss2d_exact(src, dst, lp, border, (cudaStream_t)stream, &e))
+    if (route == GaussRoute::Exact2D && gauss2d_exact(src, dst, lp, border, (cudaStream_t)stream, &e))
         return e == cudaSuccess ? NDLGPU_OK : cuda_fail(e, "exact 2-D gaussian");
     bool done = false;
-    st = gauss3d_exact(src, dst, lp, border, workspace, workspace_bytes, (cudaStream_t)stream, &done);
+    if (route == GaussRoute::Exact3D)
+        st = gauss3d_exact(src, dst, lp, border, workspace, workspace_bytes, (cudaStream_t)stream, &done);
     if (st != NDLGPU_OK || done) return st;
     return execute(c, pl, NDLGPU_ROUND_ONCE, border, workspace, workspace_bytes, (cudaStream_t)stream);
 }
@@ -1680,11 +1714,13 @@ ndlgpu_status ndlgpu_gaussian_blur_axes(const ndlgpu_view* src, const ndlgpu_vie
     Plan pl;
     st = prepare(src, dst, lp, border, NDLGPU_ROUND_ONCE, NDLGPU_PREC_AUTO, &c, &pl);
     if (st != NDLGPU_OK || c.total == 0) return st;
+    const GaussRoute route = gauss_route(src, dst, lp, pl);
     cudaError_t e = cudaSuccess;
-    if (gauss2d_exact(src, dst, lp, border, (cudaStream_t)stream, &e))
+    if (route == GaussRoute::Exact2D && gauss2d_exact(src, dst, lp, border, (cudaStream_t)stream, &e))
         return e == cudaSuccess ? NDLGPU_OK : cuda_fail(e, "exact 2-D gaussian");
     bool done = false;
-    st = gauss3d_exact(src, dst, lp, border, workspace, workspace_bytes, (cudaStream_t)stream, &done);
+    if (route == GaussRoute::Exact3D)
+        st = gauss3d_exact(src, dst, lp, border, workspace, workspace_bytes, (cudaStream_t)stream, &done);
     if (st != NDLGPU_OK || done) return st;
     return execute(c, pl, NDLGPU_ROUND_ONCE, border, workspace, workspace_bytes, (cudaStream_t)stream);
 }
@@ -2357,6 +2393,18 @@ ndlgpu_status ndlgpu_batch_info(const ndlgpu_batch* b, int* instances, int* item
 }
 
 uint64_t ndlgpu_kernel_launches(void) { return g_launches.load(std::memory_order_relaxed); }
+
+ndlgpu_status ndlgpu_test_wait_timeouts(int spin_limit, int unreachable)
+{
+    t_last_error.clear();
+    if (spin_limit < 0) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "spin_limit must be >= 0");
+    const bool on = spin_limit > 0 || unreachable != 0;
+    cudaError_t e = set_tma_wait_test(on && spin_limit > 0 ? spin_limit : (1 << 22), on && unreachable ? 16u : 0u);
+    if (e == cudaSuccess)
+        e = set_batch_wait_test(on && spin_limit > 0 ? spin_limit : (1 << 22), on && unreachable ? 1 : 0);
+    if (e != cudaSuccess) return cuda_fail(e, "wait test controls");
+    return NDLGPU_OK;
+}
 
 ndlgpu_status ndlgpu_device_status(void* stream, int32_t* code)
 {

@@ -192,6 +192,9 @@ cudaError_t launch_fused2(const FusedParams& p, cudaStream_t s);
 bool fused2_supported(int src_dtype, int dst_dtype, int kx, int ky, int kz, int adj = 0);
 // Reads and clears the fused kernels' guard word (bit 1: a plane load timed out).
 cudaError_t read_guard_fused(int32_t* v);
+// Test control of the tensor-map plane waits: poll bound and announced
+// surplus bytes (kTmaSpins and 0 restore normal operation).
+cudaError_t set_tma_wait_test(int spins, unsigned tx_bias);
 
 // Sets the per-thread message ndlgpu_last_error() returns; returns s.
 ndlgpu_status set_error(ndlgpu_status s, const std::string& msg);
@@ -420,6 +423,9 @@ cudaError_t batch_prepare(int dtype, int cfg, BatchLaunch* L);
 cudaError_t launch_batch(int dtype, int cfg, const BatchLaunch& L, cudaStream_t s);
 // Reads and clears the batched kernel's guard word (bit 2: a phase wait timed out).
 cudaError_t read_guard_batch(int32_t* v);
+// Test control of the batched phase waits: poll bound and extra
+// predecessor items asked for (1 << 22 and 0 restore normal operation).
+cudaError_t set_batch_wait_test(int spins, int need_bias);
 
 // Device guard word.
 cudaError_t read_device_status(cudaStream_t s, int32_t* code);

@@ -54,7 +54,10 @@ extern "C" ndlgpu_status ndlgpu_gaussian_blur_noalloc(const ndlgpu_view* src, co
         return set_error(NDLGPU_ERR_WORKSPACE,
                          "this blur needs " + std::to_string(need) + " bytes of scratch; the allocation-free entry "
                          "point has a fixed " + std::to_string(kScratchBytes) + " bytes");
+    // the array goes along even when the query reports no scratch: a route
+    // that needs some then finds it there (or fails with
+    // NDLGPU_ERR_WORKSPACE), and never falls back to allocating
     void* ws = nullptr;
-    if (need > 0 && (st = scratch_address(&ws)) != NDLGPU_OK) return st;
-    return ndlgpu_gaussian_blur(src, dst, sigma, border, ws, ws ? kScratchBytes : 0, stream);
+    if ((st = scratch_address(&ws)) != NDLGPU_OK) return st;
+    return ndlgpu_gaussian_blur(src, dst, sigma, border, ws, kScratchBytes, stream);
 }
