@@ -215,7 +215,7 @@ def run_gpu(args):
     kern = {}
     if not args.only:
         calls = {
-            "k_fused2 forward": fwd,
+            "k_fwd3 forward": fwd,
             "k_fused2 adjoint dL/dX": lambda: n.convolve_axes_adjoint(wi, xi, gi, passes, BorderMode.Reflect, None,
                                                                    workspace=wsa, stream=stream),
             "k_tapgrad tap gradients": lambda: n.convolve_axes_adjoint(wi, xi, None, passes, BorderMode.Reflect,
@@ -305,6 +305,14 @@ def run_gpu(args):
                "pipeline": "upload k+1 / kernels k / read-back k-1 on three streams, two device buffer sets"}
         del sets, X2, W2, Y2, G2, t2
 
+    # the batched form sharded: config 4's 512 uneven instances partitioned
+    # across the ranks by cost (ndl_b200/shard.py), each rank one persistent
+    # launch of its share; the job's time is the max over ranks (no
+    # data-path collective)
+    sharded = None
+    if not args.skip_forms:
+        sharded = sharded_config4(world, rank, dev, hbm)
+
     forms = {}
     if rank == 0 and not args.skip_forms:
         forms = other_forms(args, hbm)
@@ -322,23 +330,19 @@ def run_gpu(args):
         "metric": METRIC, "value": round(value, 3), "unit": "Gvoxel/s", "n_gpus": world, "steps": K, "warmup": Wm,
         "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded N(0,1) volumes and taps)",
-        "config": {"workload": "config 3: %d volumes of %d^3 f32 per step, per-axis 9-tap L1-normalised N(0,1) "
-                               "kernels, Reflect; forward + adjoint (dL/dX and 27 tap gradients of sum(W*Y))"
-                               % (BATCH, EDGE),
-                   "voxels_per_step": voxels, "l2": "inputs larger than L2 (226 MB per tensor)",
-                   "parallelism": "replicas%d" % world},
+        "config": step_config(world),
         "forward": {"ms": round(fwd_ms, 4), "gvoxel_s": round(voxels / fwd_ms / 1e6, 2),
                     "gbs": round(fwd_gbs, 1), "frac_of_measured_hbm": round(fwd_gbs / hbm, 4)},
         "adjoint": {"ms": round(adj_ms, 4), "gvoxel_s": round(voxels / adj_ms / 1e6, 2),
                     "gbs": round(adj_gbs, 1), "frac_of_measured_hbm": round(adj_gbs / hbm, 4)},
         "kernels": kern, "roofline": roofline, "e2e": e2e, "gpu_launches": int(launches), "clocks": sampler.result(),
-        "cpu_baseline": cpu, "forms": forms,
+        "cpu_baseline": cpu, "forms": forms, "sharded_config4": sharded,
     }
     print(json.dumps(line))
 
 
 PROFILE_OF = {
-    "k_fused2 forward": "k_fused2_fwd_f32_9x9x9_8x192cube.md",
+    "k_fwd3 forward": "k_fwd3_fwd_f32_9x9x9_8x192cube.md",
     "k_fused2 adjoint dL/dX": "k_fused2_adj_f32_9x9x9_8x192cube.md",
     "k_tapgrad tap gradients": "k_tapgrad_f32_9x9x9_8x192cube.md",
 }
@@ -487,9 +491,46 @@ def other_forms(args, hbm):
 
     out = {}
     it = max(5, min(args.steps, 20))
-    # config 2: uint8 256^3 through swap_axes(0,2).mirror(1), binomial, Wrap (x4 volumes > L2)
+    sel = getattr(args, "form", "") or ""
+
+    def want(key):
+        return not sel or key.startswith(sel) or sel.startswith(key)
+
     g = torch.Generator(device="cuda")
     g.manual_seed(SEED)
+    if want("u8_binomial"):
+        u8_form(n, g, it, hbm, out)
+    if want("gradient"):
+        gradient_form(n, g, it, hbm, out)
+    if want("gaussian_blur"):
+        gaussian_forms(n, g, it, hbm, out)
+    if want("convolve_full5x5"):
+        stencil_form(n, g, it, hbm, out)
+    if want("learnable_3tap"):
+        learnable_form(n, g, it, out)
+    if want("dog"):
+        out["dog_f32_4096^2_5scales"] = dog_form(g, it, hbm)
+    if want("downsample"):
+        downsample_form(n, g, it, hbm, out)
+    if want("box_blur"):
+        box_blur_form(n, g, it, hbm, out)
+    if want("video"):
+        video_forms(n, g, it, hbm, out, sel)
+    if want("batched"):
+        # config 4: 512 uneven instances, one persistent launch (graph replay),
+        # FP32 and BF16 storage, forward and adjoint; against the plain
+        # per-call FP32 path on the same instances
+        out.update(batched_forms(hbm))
+    if want("gauss2d"):
+        gauss2d_form(n, g, out)
+    torch.cuda.empty_cache()
+    return out
+
+
+def u8_form(n, g, it, hbm, out):
+    import torch
+    from ndl_b200 import BorderMode, Image
+    # config 2: uint8 256^3 through swap_axes(0,2).mirror(1), binomial, Wrap (x4 volumes > L2)
     base = torch.randint(0, 256, (4, 256, 256, 256), generator=g, device="cuda", dtype=torch.uint8)
     src = Image.from_tensor(base).swap_axes(0, 2).mirror(1)
     dst = Image.empty(src.extent(), torch.uint8)
@@ -502,6 +543,11 @@ def other_forms(args, hbm):
                                         "frac_of_measured_hbm": round(2.0 * vox / ms / 1e6 / hbm, 4),
                                         "exact": "bit-exact integer path"}
     del base, src, dst
+
+
+def gradient_form(n, g, it, hbm, out):
+    import torch
+    from ndl_b200 import BorderMode, Image
     # gradient (convolution.h:359-388): 256^3 f32 -> {3, 256^3} central
     # differences, Reflect; 16 algorithmic bytes per voxel (read 4, write 12)
     x = torch.randn((256, 256, 256), generator=g, device="cuda")
@@ -513,6 +559,11 @@ def other_forms(args, hbm):
                                  "gbs": round(16.0 * vox / ms / 1e6, 1),
                                  "frac_of_measured_hbm": round(16.0 * vox / ms / 1e6 / hbm, 4)}
     del x, s, o
+
+
+def gaussian_forms(n, g, it, hbm, out):
+    import torch
+    from ndl_b200 import BorderMode, Image
     # gaussian_blur of a 256^3 f32 volume (one sigma on every axis, Reflect)
     # at sigma 1, 2 and 3: the fused 3-pass kernels of 7, 13 and 19 taps
     x = torch.rand((256, 256, 256), generator=g, device="cuda")
@@ -524,6 +575,11 @@ def other_forms(args, hbm):
             "ms": round(ms, 4), "gvoxel_s": round(x.numel() / ms / 1e6, 2), "gbs": round(8.0 * x.numel() / ms / 1e6, 1),
             "frac_of_measured_hbm": round(8.0 * x.numel() / ms / 1e6 / hbm, 4)}
     del x, s, o
+
+
+def stencil_form(n, g, it, hbm, out):
+    import torch
+    from ndl_b200 import BorderMode, Image
     # convolve() with a full (non-separable) 5x5 kernel on a 4096^2 f32 image
     x = torch.rand((4096, 4096), generator=g, device="cuda")
     s = Image.from_tensor(x)
@@ -534,6 +590,11 @@ def other_forms(args, hbm):
                                           "gbs": round(8.0 * x.numel() / ms / 1e6, 1),
                                           "frac_of_measured_hbm": round(8.0 * x.numel() / ms / 1e6 / hbm, 4)}
     del x, s, o
+
+
+def learnable_form(n, g, it, out):
+    import torch
+    from ndl_b200 import BorderMode, Image
     # a learnable 3-tap-per-axis separable filter on eight 192^3 f32 volumes:
     # forward, dL/dX and the 9 tap gradients of one training step
     X = torch.randn((8, 192, 192, 192), generator=g, device="cuda")
@@ -551,7 +612,11 @@ def other_forms(args, hbm):
     out["learnable_3tap_step_f32_8x192^3"] = {"ms": round(ms, 4), "gvoxel_s": round(X.numel() / ms / 1e6, 2),
                                               "note": "forward + dL/dX + 9 tap gradients"}
     del X, W, Y, GX, xi, wi, yi, gi
-    out["dog_f32_4096^2_5scales"] = dog_form(g, it, hbm)
+
+
+def downsample_form(n, g, it, hbm, out):
+    import torch
+    from ndl_b200 import Image
     # downsample (convolution.h:241-305): a {3, 15360, 8640} uint8 colour
     # image (channel axis 0, 398 MB) by 2; algorithmic bytes = source + result
     x = torch.randint(0, 256, (8640, 15360, 3), generator=g, device="cuda", dtype=torch.uint8)
@@ -563,6 +628,11 @@ def other_forms(args, hbm):
                                               "frac_of_measured_hbm": round(nb / ms / 1e6 / hbm, 4),
                                               "exact": "bit-exact block averages"}
     del x, s, o
+
+
+def box_blur_form(n, g, it, hbm, out):
+    import torch
+    from ndl_b200 import BorderMode, Image
     # box_blur (summed_area_table.h:300-339): 4096^2 f32, radius 8, Clamp,
     # the reference's double summed-area table (bit-exact)
     x = torch.rand((4096, 4096), generator=g, device="cuda")
@@ -576,8 +646,17 @@ def other_forms(args, hbm):
                                      "exact": "bit-exact (the reference's double summed-area table, 8 B/element "
                                               "scratch written and re-read per axis)"}
     del x, s, o, ws
-    # config 5: 4-D video 1024x1024x3x96, sigma (2.5, 2.5, -, 1.5), Reflect
+
+
+def video_forms(n, g, it, hbm, out, sel=""):
+    import torch
+    from ndl_b200 import BorderMode, Image
+    from ndl_b200.convolution import gaussian_taps
+    # config 5: 4-D video 1024x1024x3x96, sigma (2.5, 2.5, -, 1.5), Reflect:
+    # the forward (gaussian_blur_axes) and the input gradient of the same chain
     for name, dt in (("video_bf16", torch.bfloat16), ("video_f16", torch.float16), ("video_f32", torch.float32)):
+        if sel and not (name.startswith(sel) or sel.startswith(name)):
+            continue
         v = torch.rand((96, 3, 1024, 1024), generator=g, device="cuda", dtype=torch.float32)
         salt = torch.rand(v.shape, generator=g, device="cuda") < 0.01
         v[salt] = 1.0
@@ -589,12 +668,20 @@ def other_forms(args, hbm):
         es = v.element_size()
         out[name] = {"ms": round(ms, 3), "gvoxel_s": round(vox / ms / 1e6, 2), "gbs": round(2.0 * es * vox / ms / 1e6, 1),
                      "frac_of_measured_hbm": round(2.0 * es * vox / ms / 1e6 / hbm, 4)}
-        del v, s, o, salt
-        out[name]["error_vs_fp64"] = video_error(dt)
-    # config 4: 512 uneven instances, one persistent launch (graph replay),
-    # FP32 and BF16 storage, forward and adjoint; against the plain per-call
-    # FP32 path on the same instances
-    out.update(batched_forms(hbm))
+        passes = [(0, gaussian_taps(2.5)), (1, gaussian_taps(2.5)), (3, gaussian_taps(1.5))]
+        ga = Image.empty(s.extent(), dt)
+        ms = time_call(lambda: n.convolve_axes_adjoint(s, None, ga, passes, BorderMode.Reflect), max(3, it // 4))
+        out[name + "_adjoint"] = {"ms": round(ms, 3), "gvoxel_s": round(vox / ms / 1e6, 2),
+                                  "gbs": round(2.0 * es * vox / ms / 1e6, 1),
+                                  "frac_of_measured_hbm": round(2.0 * es * vox / ms / 1e6 / hbm, 4)}
+        del v, s, o, salt, ga
+        if not sel:
+            out[name]["error_vs_fp64"] = video_error(dt)
+
+
+def gauss2d_form(n, g, out):
+    import torch
+    from ndl_b200 import BorderMode, Image
     # config 1: 2-D 512^2 gaussian sigma 2 (L2-resident; launch-bound)
     im = torch.rand((512, 512), generator=g, device="cuda")
     s = Image.from_tensor(im)
@@ -602,8 +689,49 @@ def other_forms(args, hbm):
     ms = time_call(lambda: n.gaussian_blur(s, o, 2.0, BorderMode.Clamp), 50)
     out["gauss2d_512_f32"] = {"ms": round(ms, 4), "gvoxel_s": round(im.numel() / ms / 1e6, 3),
                               "note": "2 MB, L2-resident and launch-bound"}
-    torch.cuda.empty_cache()
-    return out
+
+
+def sharded_config4(world, rank, dev, hbm, reps=10):
+    """Config 4 (FP32 forward) partitioned over `world` ranks by cost; every
+    rank times its own batched launch (graph replay, CUDA events) and the
+    job's time is the max over ranks."""
+    import torch
+
+    from ndl_b200 import Image
+    from ndl_b200.batch import Batch
+    from ndl_b200.shard import instance_cost, job_time_ms, partition
+
+    inst = config4_instances()
+    costs = [instance_cost(sh, [len(w) for _, w in passes]) for sh, passes, _ in inst]
+    mine = partition(costs, world)[rank]
+    g = torch.Generator(device=dev)
+    g.manual_seed(SEED + 7)
+    b = Batch()
+    keep = []
+    for i in mine:
+        sh, passes, border = inst[i]
+        x = torch.rand(sh, generator=g, device=dev)
+        y = torch.empty_like(x)
+        b.add(Image.from_tensor(x), Image.from_tensor(y), passes, border)
+        keep += [x, y]
+    b.plan()
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(3):
+        b.graph_launch(stream)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        b.graph_launch(stream)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = job_time_ms(e0.elapsed_time(e1) / reps, device=dev)
+    b.close()
+    elems = sum(int(np.prod(sh)) for sh, _, _ in inst)
+    return {"ms": round(ms, 4), "gvoxel_s": round(elems / ms / 1e6, 2), "instances": len(inst),
+            "ranks": world, "instances_this_rank": len(mine),
+            "note": "instances partitioned by cost (elements x taps) with no data-path collective; "
+                    "job time = max over ranks"}
 
 
 def config4_instances(seed=SEED):
@@ -698,6 +826,15 @@ def batched_forms(hbm, count=512, tile=None, plain=True):
 # reference has no adjoint)
 # ---------------------------------------------------------------------------
 
+def step_config(world):
+    """The workload of one step, the same for both arms (per GPU / replica)."""
+    return {"workload": "config 3: %d volumes of %d^3 f32 per step, per-axis 9-tap L1-normalised N(0,1) "
+                        "kernels, Reflect; forward + adjoint (dL/dX and 27 tap gradients of sum(W*Y))"
+                        % (BATCH, EDGE),
+            "voxels_per_step": BATCH * EDGE ** 3, "l2": "inputs larger than L2 (226 MB per tensor)",
+            "parallelism": "replicas%d" % world}
+
+
 def _cpu_model():
     try:
         with open("/proc/cpuinfo") as f:
@@ -744,22 +881,22 @@ def cpu_baseline_sample(volumes=5):
 
 
 def run_reference(args):
-    """--impl reference: the reference's own CPU path on all host threads
-    (independent samples in parallel; ndl's convolve() is single-threaded and
-    re-entrant, processing/convolution.h:64-70)."""
+    """--impl reference: the reference's own CPU path on the host cores, on
+    the GPU arm's step (BATCH volumes of 192^3): one volume per thread, the
+    volumes in parallel (ndl's convolve() is single-threaded and re-entrant,
+    processing/convolution.h:64-70)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     from concurrent.futures import ThreadPoolExecutor
-    cores = os.cpu_count() or 1
-    depth = 8
+    threads = min(os.cpu_count() or 1, BATCH)
     K, Wm = args.steps, max(3, args.warmup)
+    ex = ThreadPoolExecutor(threads)
 
     def step():
         t0 = time.perf_counter()
-        with ThreadPoolExecutor(cores) as ex:
-            res = list(ex.map(lambda i: cpu_sample(depth, SEED + i), range(cores)))
+        res = list(ex.map(lambda i: cpu_sample(EDGE, SEED + i), range(BATCH)))
         dt = time.perf_counter() - t0
         return sum(r[0] for r in res), dt, res[0][2]
 
@@ -770,15 +907,16 @@ def run_reference(args):
         v, s, kind = step()
         vox += v
         sec += s
+    ex.shutdown()
     value = vox / sec / 1e9
     line = {"impl": "reference", "metric": METRIC, "value": round(value, 6), "unit": "Gvoxel/s", "n_gpus": world,
             "steps": K, "warmup": Wm, "ms_per_step": round(1e3 * sec / K, 2), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "config 3 per-voxel work (192x192 planes, 9-tap x3, Reflect, fwd+adjoint)"},
-            "cpu_baseline": {"value": round(value, 6), "unit": "Gvoxel/s", "cores": cores, "kind": kind,
-                             "sample": "%d threads, each a 192x192x%d f32 volume per step: forward = ndl convolve() x3 "
-                                       "(compiled reference) + adjoint = FP64 oracle port; %s"
-                                       % (cores, depth, _cpu_model())},
+            "config": step_config(world),
+            "cpu_baseline": {"value": round(value, 6), "unit": "Gvoxel/s", "cores": threads, "kind": kind,
+                             "sample": "every step the GPU arm's %d volumes of 192^3 f32, one per thread on %d "
+                                       "threads: forward = ndl convolve() x3 (compiled reference) + adjoint = "
+                                       "FP64 oracle port (ndl has no adjoint); %s" % (BATCH, threads, _cpu_model())},
             "e2e": {"value": round(value, 6), "unit": "Gvoxel/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -797,9 +935,15 @@ def main():
     ap.add_argument("--batched-tile", type=int, default=None, help="tile configuration instead of the autotuner")
     ap.add_argument("--only", default="", choices=["", "fwd", "adj"],
                     help="time only one half of the step (for profiling captures)")
+    ap.add_argument("--form", default="",
+                    help="run only the other form(s) whose name starts with this (e.g. video_bf16, gradient, "
+                         "u8_binomial, convolve_full5x5): for profiling captures; prints their timings")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.form:
+        hbm, _ = peaks()
+        print(json.dumps(other_forms(args, hbm)))
     elif args.batched_only:
         hbm, _ = peaks()
         print(json.dumps(batched_forms(hbm, args.batched_only, args.batched_tile, plain=False)))

@@ -122,9 +122,13 @@ __global__ void __launch_bounds__(NT, 1) k_fused(const __grid_constant__ FusedPa
     }
 
     A stage[NLD];
+    // copies of the parameters the plane loads read (a lambda reading the
+    // __grid_constant__ parameters through a reference would make generic loads)
+    const int l_border = p.border, l_nz = p.nz;
+    const int64_t l_sz = p.sz;
     auto fetch = [&](int zi) {
-        const int zm = map_border32(p.border, p.nz, zi);
-        const Tin* pl = src + (int64_t)zm * p.sz;
+        const int zm = map_border32(l_border, l_nz, zi);
+        const Tin* pl = src + (int64_t)zm * l_sz;
 #pragma unroll
         for (int j = 0; j < NLD; j++)
             if (tid + j * NT < ROWS * COLS) stage[j] = to_acc<Tin, A>(pl[loff[j]]);

@@ -184,11 +184,12 @@ cudaError_t read_guard_generic(int32_t* v)
 namespace ndlgpu {
 cudaError_t read_device_status(cudaStream_t, int32_t* code)
 {
-    int32_t a = 0, b = 0, c = 0;
+    int32_t a = 0, b = 0, c = 0, d = 0;
     cudaError_t e = read_guard_generic(&a);
     if (e == cudaSuccess) e = read_guard_fused(&b);
     if (e == cudaSuccess) e = read_guard_batch(&c);
-    *code = a | b | c;
+    if (e == cudaSuccess) e = read_guard_fwd3(&d);
+    *code = a | b | c | d;
     return e;
 }
 }  // namespace ndlgpu

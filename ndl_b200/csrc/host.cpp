@@ -670,10 +670,14 @@ static ndlgpu_status execute(const Canon& c, const Plan& pl, int compose, int bo
 {
     if (c.total == 0) return NDLGPU_OK;
     if (pl.fused) {
-        cudaError_t e = (pl.acc == Acc::F32 && fused2_supported(pl.fp.src_dtype, pl.fp.dst_dtype, pl.fp.kx, pl.fp.ky,
-                                                                 pl.fp.kz))
-                            ? launch_fused2(pl.fp, s)
-                            : launch_fused(pl.acc, pl.fp, s);
+        const FusedParams& f = pl.fp;
+        cudaError_t e;
+        if (pl.acc == Acc::F32 && !f.adj && !f.tstore && fwd3_supported(f.src_dtype, f.dst_dtype, f.kx, f.ky, f.kz))
+            e = launch_fwd3(f, s);
+        else if (pl.acc == Acc::F32 && fused2_supported(f.src_dtype, f.dst_dtype, f.kx, f.ky, f.kz))
+            e = launch_fused2(f, s);
+        else
+            e = launch_fused(pl.acc, f, s);
         if (e != cudaSuccess) return cuda_fail(e, "fused kernel");
         return NDLGPU_OK;
     }
@@ -2400,6 +2404,9 @@ ndlgpu_status ndlgpu_test_wait_timeouts(int spin_limit, int unreachable)
     if (spin_limit < 0) return fail(NDLGPU_ERR_INVALID_ARGUMENT, "spin_limit must be >= 0");
     const bool on = spin_limit > 0 || unreachable != 0;
     cudaError_t e = set_tma_wait_test(on && spin_limit > 0 ? spin_limit : (1 << 22), on && unreachable ? 16u : 0u);
+    if (e == cudaSuccess)
+        e = set_fwd3_wait_test(on && spin_limit > 0 ? spin_limit : (1 << 22), on && unreachable ? 16u : 0u);
+
     if (e == cudaSuccess)
         e = set_batch_wait_test(on && spin_limit > 0 ? spin_limit : (1 << 22), on && unreachable ? 1 : 0);
     if (e != cudaSuccess) return cuda_fail(e, "wait test controls");

@@ -190,6 +190,13 @@ bool fused_supported(Acc acc, int src_dtype, int dst_dtype, int kx, int ky, int 
 // Float-storage fused kernel with asynchronous loads (fused2.cu).
 cudaError_t launch_fused2(const FusedParams& p, cudaStream_t s);
 bool fused2_supported(int src_dtype, int dst_dtype, int kx, int ky, int kz, int adj = 0);
+// Fused forward of a volume, Y pass first with every pass packed (fwd3.cu).
+cudaError_t launch_fwd3(const FusedParams& p, cudaStream_t s);
+bool fwd3_supported(int src_dtype, int dst_dtype, int kx, int ky, int kz);
+// Reads and clears its guard word (bit 1: a tensor-map plane wait timed out),
+// and sets the test controls of those waits (1 << 22 and 0: normal).
+cudaError_t read_guard_fwd3(int32_t* v);
+cudaError_t set_fwd3_wait_test(int spins, unsigned tx_bias);
 // Reads and clears the fused kernels' guard word (bit 1: a plane load timed out).
 cudaError_t read_guard_fused(int32_t* v);
 // Test control of the tensor-map plane waits: poll bound and announced
@@ -247,6 +254,7 @@ bool tapgrad_supported(int dt, int kx, int ky, int kz);
 long long tapgrad_ctas(const TapFusedParams& p);
 int tapgrad_zchunk(int nx, int ny, int nz, int nbatch, int kz);
 cudaError_t launch_tapgrad(const TapFusedParams& p, void* out, int out_dtype, const TapFinalMap& mp, cudaStream_t s);
+
 
 // gradient (gradient.cu): all DIM central differences of a voxel in one pass.
 struct GradParams {

@@ -1,7 +1,7 @@
 """Bounded device waits that run out, without any fault.
 
-The tensor-map plane loads of the fused adjoint and the phase waits of the
-batched form poll a bounded number of times; when the bound is reached the
+The tensor-map plane loads of the fused forward and adjoint and the phase
+waits of the batched form poll a bounded number of times; when the bound is reached the
 kernel sets a guard bit, lets its own copies in flight land and returns, and
 ndlgpu_device_status reports the bit.  ndlgpu_test_wait_timeouts makes those
 waits ask for more than ever arrives (an mbarrier announced 16 bytes more
@@ -43,7 +43,9 @@ def _passes(rng, k=9):
 
 def test_tensor_map_plane_wait_runs_out_and_reports():
     rng = np.random.default_rng(3)
-    g = rng.standard_normal((40, 48, 72)).astype(np.float32)
+    # rows of 64 elements: whole 64-column tiles, so the plane loads go
+    # through the tensor map
+    g = rng.standard_normal((40, 48, 64)).astype(np.float32)
     passes = _passes(rng)
     gi = Image.from_tensor(torch.from_numpy(g).cuda())
     gx = Image.empty(gi.extent(), torch.float32)
@@ -64,6 +66,29 @@ def test_tensor_map_plane_wait_runs_out_and_reports():
         ref = O.axis_pass_adjoint(ref, ax, w, O.REFLECT)
     err = np.abs(gx.tensor().cpu().numpy() - ref).max() / np.abs(ref).max()
     assert err <= 1e-5, err
+
+
+def test_forward_plane_wait_runs_out_and_reports():
+    # the forward's tensor-map plane loads (64-wide rows, Reflect)
+    rng = np.random.default_rng(6)
+    x = rng.standard_normal((24, 32, 64)).astype(np.float32)
+    passes = _passes(rng)
+    xi = Image.from_tensor(torch.from_numpy(x).cuda())
+    y = Image.empty(xi.extent(), torch.float32)
+    assert _status() == 0
+    _controls(64, 1)
+    try:
+        n.convolve_axes(xi, y, passes, n.BorderMode.Reflect)
+        code = _status()
+    finally:
+        _controls(0, 0)
+    assert code & 2, code
+    n.convolve_axes(xi, y, passes, n.BorderMode.Reflect)
+    torch.cuda.synchronize()
+    assert _status() == 0
+    ref = O.compose_total(x.astype(np.float64), passes, O.REFLECT)
+    mag = O.compose_total(np.abs(x).astype(np.float64), [(a, np.abs(w)) for a, w in passes], O.REFLECT)
+    assert (np.abs(y.tensor().cpu().numpy() - ref) <= 1e-6 * mag + 1e-30).all()
 
 
 def test_batched_phase_wait_runs_out_and_reports():
