@@ -715,7 +715,9 @@ def sharded_config4(world, rank, dev, hbm, reps=10):
         b.add(Image.from_tensor(x), Image.from_tensor(y), passes, border)
         keep += [x, y]
     b.plan()
-    stream = torch.cuda.current_stream(dev)
+    # graph capture needs a stream other than the legacy default one
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.synchronize(dev)
     for _ in range(3):
         b.graph_launch(stream)
     torch.cuda.synchronize(dev)
