@@ -540,7 +540,8 @@ static bool plan_fused(const Canon& c, Acc acc, int compose, int border, FusedPa
     if (role[2] >= 0 && !dense(by_axis[role[2]], &kz)) return false;
     const bool v2 = (acc == Acc::F32) && fused2_supported(c.sdt, c.ddt, kx, ky, kz, adj);
     if (adj && !v2) return false;
-    if (!v2 && !fused_supported(acc, c.sdt, c.ddt, kx, ky, kz)) return false;
+    const bool u8shape = acc == Acc::I32 && !adj && fused_u8_shape(c.sdt, c.ddt, kx, ky, kz);
+    if (!v2 && !fused_supported(acc, c.sdt, c.ddt, kx, ky, kz) && !u8shape) return false;
 
     FusedParams& p = *fp;
     std::memset(&p, 0, sizeof(p));
@@ -634,6 +635,8 @@ static bool plan_fused(const Canon& c, Acc acc, int compose, int border, FusedPa
     p.vec_st = (p.dx == 1 && al(p.dst, 4 * des) && (p.dy % 4) == 0 && (p.dz % 4) == 0 && (p.db % 4) == 0) ? 1 : 0;
     p.vec_st = v2 ? p.vec_st : 0;
     p.tstore = tstore ? 1 : 0;
+    // a shape only the packed uint8 kernel compiles must also meet its bounds
+    if (u8shape && !fused_supported(acc, c.sdt, c.ddt, kx, ky, kz) && !fused_u8_supported(p)) return false;
     // Z chunk of the integer kernel (64 x 32 tiles, two resident CTAs per SM);
     // the float kernel picks its own at launch
     int dev = 0, sms = 148;
@@ -676,6 +679,8 @@ static ndlgpu_status execute(const Canon& c, const Plan& pl, int compose, int bo
             e = launch_fwd3(f, s);
         else if (pl.acc == Acc::F32 && fused2_supported(f.src_dtype, f.dst_dtype, f.kx, f.ky, f.kz))
             e = launch_fused2(f, s);
+        else if (pl.acc == Acc::I32 && fused_u8_supported(f))
+            e = launch_fused_u8(f, s);
         else
             e = launch_fused(pl.acc, f, s);
         if (e != cudaSuccess) return cuda_fail(e, "fused kernel");

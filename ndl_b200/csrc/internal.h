@@ -190,6 +190,12 @@ bool fused_supported(Acc acc, int src_dtype, int dst_dtype, int kx, int ky, int 
 // Float-storage fused kernel with asynchronous loads (fused2.cu).
 cudaError_t launch_fused2(const FusedParams& p, cudaStream_t s);
 bool fused2_supported(int src_dtype, int dst_dtype, int kx, int ky, int kz, int adj = 0);
+// Fused forward of a uint8 volume with non-negative dyadic integer taps,
+// two values packed per 32-bit word (fused_u8.cu): the compiled tap counts,
+// and whether a planned launch qualifies (taps, bounds, layout).
+bool fused_u8_shape(int sdt, int ddt, int kx, int ky, int kz);
+bool fused_u8_supported(const FusedParams& p);
+cudaError_t launch_fused_u8(const FusedParams& p, cudaStream_t s);
 // Fused forward of a volume, Y pass first with every pass packed (fwd3.cu).
 cudaError_t launch_fwd3(const FusedParams& p, cudaStream_t s);
 bool fwd3_supported(int src_dtype, int dst_dtype, int kx, int ky, int kz);
