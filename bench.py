@@ -565,11 +565,12 @@ def gaussian_forms(n, g, it, hbm, out):
     import torch
     from ndl_b200 import BorderMode, Image
     # gaussian_blur of a 256^3 f32 volume (one sigma on every axis, Reflect)
-    # at sigma 1, 2 and 3: the fused 3-pass kernels of 7, 13 and 19 taps
+    # at sigma 1, 2 and 3: the fused 3-pass kernels of 7, 13 and 19 taps; at
+    # sigma 4 and 6 (25 and 37 taps): three tiled passes through f32 scratch
     x = torch.rand((256, 256, 256), generator=g, device="cuda")
     s = Image.from_tensor(x)
     o = Image.empty(s.extent(), torch.float32)
-    for sg in (1.0, 2.0, 3.0):
+    for sg in (1.0, 2.0, 3.0, 4.0, 6.0):
         ms = time_call(lambda: n.gaussian_blur(s, o, sg, BorderMode.Reflect), it)
         out["gaussian_blur_f32_256^3_sigma%g" % sg] = {
             "ms": round(ms, 4), "gvoxel_s": round(x.numel() / ms / 1e6, 2), "gbs": round(8.0 * x.numel() / ms / 1e6, 1),

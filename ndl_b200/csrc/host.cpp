@@ -8,6 +8,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -309,6 +310,37 @@ struct Scratch {
 
 static size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
 
+// The library's own stream-ordered pool for scratch the caller did not
+// provide, one per device: it keeps up to 2 GiB cached between calls (the
+// device's default pool returns everything at each synchronisation, so every
+// call would map its scratch anew); the process's other pools are untouched.
+static cudaError_t scratch_pool(cudaMemPool_t* out)
+{
+    static std::mutex mu;
+    static std::vector<cudaMemPool_t> pools;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    if ((int)pools.size() <= dev) pools.resize(dev + 1, nullptr);
+    if (!pools[dev]) {
+        cudaMemPoolProps props;
+        std::memset(&props, 0, sizeof(props));
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool;
+        e = cudaMemPoolCreate(&pool, &props);
+        if (e != cudaSuccess) return e;
+        uint64_t keep = 2ull << 30;
+        e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (e != cudaSuccess) return e;
+        pools[dev] = pool;
+    }
+    *out = pools[dev];
+    return cudaSuccess;
+}
+
 static ndlgpu_status get_scratch(size_t need, void* ws, size_t ws_bytes, cudaStream_t s, Scratch* sc)
 {
     if (need == 0) return NDLGPU_OK;
@@ -319,8 +351,11 @@ static ndlgpu_status get_scratch(size_t need, void* ws, size_t ws_bytes, cudaStr
         sc->base = ws;
         return NDLGPU_OK;
     }
-    cudaError_t e = cudaMallocAsync(&sc->base, need, s);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaMallocAsync(workspace)");
+    cudaMemPool_t pool = nullptr;
+    cudaError_t e = scratch_pool(&pool);
+    if (e != cudaSuccess) return cuda_fail(e, "scratch memory pool");
+    e = cudaMallocFromPoolAsync(&sc->base, need, pool, s);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMallocFromPoolAsync(workspace)");
     sc->owned = true;
     sc->stream = s;
     return NDLGPU_OK;
@@ -344,6 +379,37 @@ static ndlgpu_status run_generic_pass(Acc acc, const Canon& c, const CPass& pass
                                       cudaStream_t s, bool transpose = false)
 {
     const int R = (int)c.ax.size();
+    // float storage with FP32 sums and dense taps: the tiled pass kernels
+    if (!transpose && acc == Acc::F32 && store_mode == STORE_CAST && R <= kTiledRank && !pass.off.empty() &&
+        (int)pass.off.size() <= kMaxTaps) {
+        TiledPassParams t;
+        std::memset(&t, 0, sizeof(t));
+        std::vector<std::pair<int, double>> tw;
+        for (size_t i = 0; i < pass.off.size(); i++) tw.push_back({pass.off[i], pass.w[i]});
+        std::sort(tw.begin(), tw.end());
+        t.src = in;
+        t.dst = out;
+        t.src_dtype = in_dt;
+        t.dst_dtype = out_dt;
+        t.rank = R;
+        t.axis = pass.axis;
+        t.border = border;
+        t.ntap = (int)tw.size();
+        t.omin = tw.front().first;
+        t.omax = tw.back().first;
+        for (int k = 0; k < t.ntap; k++) t.w[k] = (float)tw[k].second;
+        for (int i = 0; i < R; i++) {
+            t.n[i] = c.ax[i].n;
+            t.ss[i] = in_st[i];
+            t.ds[i] = out_st[i];
+        }
+        t.rows = c.total / c.ax[0].n;
+        if (tiled_pass_supported(t)) {
+            cudaError_t e = launch_tiled_pass(t, s);
+            if (e != cudaSuccess) return cuda_fail(e, "tiled pass");
+            return NDLGPU_OK;
+        }
+    }
     GenericPassParams p;
     std::memset(&p, 0, sizeof(p));
     p.src_dtype = in_dt;

@@ -100,6 +100,25 @@ struct GenericPassParams {
     int32_t wi[kMaxTaps];
 };
 
+// One pass of any width along one axis, FP32 accumulation, float storage
+// (pass_tiled.cu): canonical axes (0 = x, contiguous in neither necessarily),
+// dense taps at offsets omin .. omax in ascending order.
+constexpr int kTiledRank = 4;
+struct TiledPassParams {
+    const char* src;
+    char* dst;
+    int src_dtype, dst_dtype;
+    int rank, axis, border;
+    int ntap, omin, omax;
+    int64_t rows;                 // product of the extents of every axis but 0
+    int64_t n[kTiledRank], ss[kTiledRank], ds[kTiledRank];
+    FastDiv dv[kTiledRank];       // dividers of the extents, and of the tile count along x
+    FastDiv dtx;
+    float w[kMaxTaps];
+};
+bool tiled_pass_supported(const TiledPassParams& p);
+cudaError_t launch_tiled_pass(const TiledPassParams& p, cudaStream_t s);
+
 // The general N-D kernel (non-separable convolve()): taps live in device
 // memory as ntap records of rank int32 offsets plus a double weight.
 struct GenericNdParams {
