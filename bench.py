@@ -252,7 +252,7 @@ def run_gpu(args):
         hY = torch.empty_like(hX, pin_memory=True)
         hG = torch.empty_like(hX, pin_memory=True)
         htaps = torch.empty(3 * NTAP, dtype=torch.float32, pin_memory=True)
-        ke = max(3, min(K, 10))
+        ke = max(3, min(K, 24))   # steps timed: pipeline fill and drain amortised over them
         sets = [(X, W, Y, GX, taps, xi, wi, yi, gi)]
         X2, W2, Y2, G2 = (torch.empty_like(X) for _ in range(4))
         t2 = torch.zeros_like(taps)

@@ -72,7 +72,17 @@ __global__ void __launch_bounds__(NT) k_tpass_x(const __grid_constant__ TiledPas
     if (row < nrows) outer_offsets(p, 0, -1, row, &so, &dof);
     const Tin* src = reinterpret_cast<const Tin*>(p.src) + so;
     float* srow = sm_x + warp * pitch;
-    if (row < nrows) {
+    // rows wholly inside the image, 16-byte aligned f32: float4 loads
+    const int nvec = (XO + K - 1 + 3) >> 2;
+    bool vec = false;
+    if constexpr (sizeof(Tin) == 4)
+        vec = p.ss[0] == 1 && x0 + p.omin >= 0 && x0 + p.omin + 4 * nvec <= n0 &&
+              (reinterpret_cast<uintptr_t>(src + x0 + p.omin) & 15) == 0;
+    if (row < nrows && vec) {
+        const float4* v4 = reinterpret_cast<const float4*>(src + x0 + p.omin);
+#pragma unroll 2
+        for (int v = lane; v < nvec; v += 32) *reinterpret_cast<float4*>(srow + 4 * v) = v4[v];
+    } else if (row < nrows) {
         // unrolled so that the loads of several iterations are in flight at once
 #pragma unroll 4
         for (int j = lane; j < pitch; j += 32) {
@@ -132,6 +142,20 @@ __global__ void __launch_bounds__(NT) k_tpass_s(const __grid_constant__ TiledPas
     for (int i = tid; i < K; i += NT) s_w[i] = p.w[i];
     // staged rows r = 0 .. nr-1: axis coordinate y0 + omin + r, border-mapped;
     // columns x0 .. x0+63 (past n0: zero, never stored)
+    // rows of 64 columns inside the image, 16-byte aligned f32: float4 loads
+    bool vec = false;
+    if constexpr (sizeof(Tin) == 4)
+        vec = p.ss[0] == 1 && x0 + SC <= n0 && (p.ss[a] & 3) == 0 && (reinterpret_cast<uintptr_t>(src + x0) & 15) == 0;
+    if (vec) {
+#pragma unroll 4
+        for (int i = tid; i < nr * (SC / 4); i += NT) {
+            const int r = i / (SC / 4), c4 = i - (i / (SC / 4)) * (SC / 4);
+            int64_t y = y0 + p.omin + r;
+            if (y < 0 || y >= na) y = (y >= na + p.omax || y < p.omin) ? na - 1 : bmap(p.border, na, y);
+            *reinterpret_cast<float4*>(sm_s + r * SC + 4 * c4) =
+                *reinterpret_cast<const float4*>(src + x0 + 4 * c4 + y * p.ss[a]);
+        }
+    } else
     // (unrolled so that the loads of several iterations are in flight at once)
 #pragma unroll 8
     for (int i = tid; i < nr * SC; i += NT) {
