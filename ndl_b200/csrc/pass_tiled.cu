@@ -5,13 +5,15 @@
 //
 // The tile (outputs plus the tap window) is staged in shared memory with its
 // coordinates border-mapped (Clamp / Wrap / Reflect, mathHelpers.h:23-25),
-// then every thread sums four outputs, four taps at a time from a register
-// window, and the last K mod 4 taps one by one (no tap past the kernel is
-// ever read, so non-finite samples behave as in the reference's sum):
-//   along x (the contiguous axis): 8 rows x 128 outputs per CTA, a warp per
-//     row, lane l outputs 4l .. 4l+3;
-//   along another axis: 64 columns x 32 outputs per CTA, a thread a column
-//     pair (packed FP32 pairs) and 4 outputs along the axis.
+// then every thread sums its outputs from a sliding register window, taps in
+// ascending order (no tap past the kernel is ever multiplied, so non-finite
+// samples behave as in the reference's sum):
+//   along x (the contiguous axis): 8 rows x 256 outputs per CTA, a warp per
+//     row, lane l outputs 4l .. 4l+3 and 128+4l .. 128+4l+3, four taps per
+//     step from two 16-byte chunks per output block;
+//   along another axis: 64 columns x 64 outputs per CTA, a thread a column
+//     pair (packed FP32 pairs) and 8 outputs along the axis, one new row per
+//     tap.
 // Taps are the pass's dense offsets omin .. omin+K-1 in ascending order.
 #include "dtype.cuh"
 
@@ -19,10 +21,10 @@ namespace ndlgpu {
 namespace {
 
 constexpr int NT = 256;
-constexpr int XO = 128;     // x pass: outputs per row
+constexpr int XO = 256;     // x pass: outputs per row
 constexpr int XR = 8;       // x pass: rows per CTA
 constexpr int SC = 64;      // strided pass: columns per CTA
-constexpr int SO = 32;      // strided pass: outputs along the axis per CTA
+constexpr int SO = 64;      // strided pass: outputs along the axis per CTA
 
 template <class T> __device__ __forceinline__ float ldf(const T* p);
 template <> __device__ __forceinline__ float ldf<float>(const float* p) { return *p; }
@@ -54,83 +56,157 @@ __device__ __forceinline__ void outer_offsets(const TiledPassParams& p, int skip
     *dof = d;
 }
 
+// x pass: the window of row `row` from x0 + omin, Lr floats (the outputs'
+// XO + K - 1 plus the chunk the last step reads past it), staged so that
+// srow[j] holds the input at x0 + omin + j.  Global reads are 16-byte chunks
+// aligned down from x0 + omin (rem = the offset into the first chunk); chunks
+// wholly inside a contiguous f32 row load as float4, the rest (the row's ends,
+// strided or 16-bit rows) element by element with their coordinates mapped.
+__host__ __device__ constexpr int x_window(int K) { return (XO + K + 4 + 3) & ~3; }
+__host__ __device__ constexpr int x_pitch(int K) { return x_window(K) + 8; }
+
+// Four taps on four outputs from an 8-float register window (chunks A, B).
+__device__ __forceinline__ void taps4(float (&a)[4], const float4 A, const float4 B, const float4 w)
+{
+    const float win[8] = {A.x, A.y, A.z, A.w, B.x, B.y, B.z, B.w};
+    const float wq[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+#pragma unroll
+        for (int m = 0; m < 4; m++) a[m] = fmaf(wq[q], win[m + q], a[m]);
+}
+
+// The last r (1..3) taps: the same window, taps 0 .. r-1 only.
+__device__ __forceinline__ void taps_tail(float (&a)[4], const float4 A, const float4 B, const float4 w, int r)
+{
+    const float win[8] = {A.x, A.y, A.z, A.w, B.x, B.y, B.z, B.w};
+    const float wq[3] = {w.x, w.y, w.z};
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        if (q >= r) break;
+#pragma unroll
+        for (int m = 0; m < 4; m++) a[m] = fmaf(wq[q], win[m + q], a[m]);
+    }
+}
+
 template <class Tin, class Tout>
 __global__ void __launch_bounds__(NT) k_tpass_x(const __grid_constant__ TiledPassParams p)
 {
     extern __shared__ __align__(16) float sm_x[];
     const int K = p.ntap;
-    const int pitch = (XO + K + 3 + 3) & ~3;       // the last lane's window reads up to XO + K + 2
-    float* s_w = sm_x + XR * pitch;
+    const int L = x_window(K);
+    float* s_w = sm_x + XR * x_pitch(K);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int64_t n0 = p.n[0];
     const uint32_t rb = p.dtx.div(blockIdx.x), tx = blockIdx.x - rb * p.dtx.d;
     const int64_t x0 = (int64_t)tx * XO;
     const uint32_t nrows = (uint32_t)p.rows;
-    for (int i = tid; i < K; i += NT) s_w[i] = p.w[i];
+    const int K4 = (K + 3) & ~3;
+    for (int i = tid; i < K4; i += NT) s_w[i] = i < K ? p.w[i] : 0.f;
     const uint32_t row = rb * XR + warp;
     int64_t so = 0, dof = 0;
     if (row < nrows) outer_offsets(p, 0, -1, row, &so, &dof);
     const Tin* src = reinterpret_cast<const Tin*>(p.src) + so;
-    float* srow = sm_x + warp * pitch;
-    // rows wholly inside the image, 16-byte aligned f32: float4 loads
-    const int nvec = (XO + K - 1 + 3) >> 2;
-    bool vec = false;
-    if constexpr (sizeof(Tin) == 4)
-        vec = p.ss[0] == 1 && x0 + p.omin >= 0 && x0 + p.omin + 4 * nvec <= n0 &&
-              (reinterpret_cast<uintptr_t>(src + x0 + p.omin) & 15) == 0;
-    if (row < nrows && vec) {
-        const float4* v4 = reinterpret_cast<const float4*>(src + x0 + p.omin);
-#pragma unroll 2
-        for (int v = lane; v < nvec; v += 32) *reinterpret_cast<float4*>(srow + 4 * v) = v4[v];
-    } else if (row < nrows) {
-        // unrolled so that the loads of several iterations are in flight at once
-#pragma unroll 4
-        for (int j = lane; j < pitch; j += 32) {
-            float v = 0.f;
-            if (j < XO + K - 1) {
-                int64_t x = x0 + p.omin + j;
-                if (x < 0 || x >= n0) x = (x >= n0 + p.omax || x < p.omin) ? n0 - 1 : bmap(p.border, n0, x);
-                v = ldf<Tin>(src + x * p.ss[0]);
+    float* srow = sm_x + warp * x_pitch(K) + 4;
+    if (row < nrows) {
+        // coordinates fit 32 bits (extents below 2^30)
+        const int n0i = (int)n0;
+        const int gs = (int)x0 + p.omin;
+        const int xs = gs & ~3;
+        const int rem = gs - xs;
+        const int nv = (L + rem + 3) >> 2;
+        // chunks va .. vb-1 lie wholly inside [0, n0) and load as float4
+        int va = 0, vb = 0;
+        if constexpr (sizeof(Tin) == 4) {
+            if (p.ss[0] == 1 && (reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+                va = min(nv, xs >= 0 ? 0 : -xs >> 2);
+                vb = max(va, min(nv, (n0i - xs) >> 2));
             }
-            srow[j] = v;
+            const float* s4 = reinterpret_cast<const float*>(src) + xs;
+#pragma unroll 3
+            for (int v = va + lane; v < vb; v += 32) {
+                const float4 t = *reinterpret_cast<const float4*>(s4 + 4 * v);
+                float* d = srow + 4 * v - rem;
+                if (rem == 0) {
+                    *reinterpret_cast<float4*>(d) = t;
+                } else if (rem == 2) {
+                    *reinterpret_cast<float2*>(d) = make_float2(t.x, t.y);
+                    *reinterpret_cast<float2*>(d + 2) = make_float2(t.z, t.w);
+                } else {
+                    d[0] = t.x;
+                    *reinterpret_cast<float2*>(d + 1) = make_float2(t.y, t.z);
+                    d[3] = t.w;
+                }
+            }
+        }
+        // every other element of the window (the row's ends, or the whole
+        // window of a strided or 16-bit row): coordinates border-mapped
+        const int nlead = 4 * va, nrest = nlead + 4 * (nv - vb);
+        for (int i = lane; i < nrest; i += 32) {
+            const int e = i < nlead ? i : 4 * vb + (i - nlead);
+            int x = xs + e;
+            if (x < 0 || x >= n0i) x = (x >= n0i + p.omax || x < p.omin) ? n0i - 1 : map_border32(p.border, n0i, x);
+            srow[e - rem] = ldf<Tin>(src + (int64_t)x * p.ss[0]);
         }
     }
     __syncthreads();
     if (row >= nrows) return;
-    float a[4] = {0.f, 0.f, 0.f, 0.f};
-    const float* wr = srow + 4 * lane;
-    const int K4 = K & ~3;
-    for (int t = 0; t < K4; t += 4) {
-        const float4 v0 = *reinterpret_cast<const float4*>(wr + t);
-        const float4 v1 = *reinterpret_cast<const float4*>(wr + t + 4);
-        const float4 w = *reinterpret_cast<const float4*>(s_w + t);
-        const float win[8] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w};
-        const float wq[4] = {w.x, w.y, w.z, w.w};
-#pragma unroll
-        for (int q = 0; q < 4; q++)
-#pragma unroll
-            for (int m = 0; m < 4; m++) a[m] = fmaf(wq[q], win[m + q], a[m]);
+    // lane l: outputs 4l .. 4l+3 and 128+4l .. 128+4l+3 (16-byte lane stride:
+    // conflict-free window reads); a sliding window of two chunks per block
+    const float* b0 = srow + 4 * lane;
+    const float* b1 = b0 + XO / 2;
+    float a0[4] = {0.f, 0.f, 0.f, 0.f}, a1[4] = {0.f, 0.f, 0.f, 0.f};
+    float4 A0 = *reinterpret_cast<const float4*>(b0), A1 = *reinterpret_cast<const float4*>(b1);
+    const int S = K >> 2;
+#pragma unroll 2
+    for (int s = 0; s < S; s++) {
+        const float4 B0 = *reinterpret_cast<const float4*>(b0 + 4 * s + 4);
+        const float4 B1 = *reinterpret_cast<const float4*>(b1 + 4 * s + 4);
+        const float4 w = *reinterpret_cast<const float4*>(s_w + 4 * s);
+        taps4(a0, A0, B0, w);
+        taps4(a1, A1, B1, w);
+        A0 = B0;
+        A1 = B1;
     }
-    for (int t = K4; t < K; t++) {
-        const float w = s_w[t];
-#pragma unroll
-        for (int m = 0; m < 4; m++) a[m] = fmaf(w, wr[m + t], a[m]);
+    if (K & 3) {
+        const float4 B0 = *reinterpret_cast<const float4*>(b0 + 4 * S + 4);
+        const float4 B1 = *reinterpret_cast<const float4*>(b1 + 4 * S + 4);
+        const float4 w = *reinterpret_cast<const float4*>(s_w + 4 * S);
+        taps_tail(a0, A0, B0, w, K & 3);
+        taps_tail(a1, A1, B1, w, K & 3);
     }
     Tout* dst = reinterpret_cast<Tout*>(p.dst) + dof;
+    bool vst = false;
+    if constexpr (sizeof(Tout) == 4) vst = p.ds[0] == 1 && (reinterpret_cast<uintptr_t>(dst) & 15) == 0;
 #pragma unroll
-    for (int m = 0; m < 4; m++) {
-        const int64_t x = x0 + 4 * lane + m;
-        if (x < n0) dst[x * p.ds[0]] = stf<Tout>(a[m]);
+    for (int h = 0; h < 2; h++) {
+        const float* a = h ? a1 : a0;
+        const int64_t xb = x0 + 4 * lane + h * (XO / 2);
+        if constexpr (sizeof(Tout) == 4) {
+            if (vst && xb + 4 <= n0) {
+                *reinterpret_cast<float4*>(reinterpret_cast<float*>(dst) + xb) = make_float4(a[0], a[1], a[2], a[3]);
+                continue;
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < 4; m++)
+            if (xb + m < n0) dst[(xb + m) * p.ds[0]] = stf<Tout>(a[m]);
     }
 }
 
+// Strided pass (any axis but x): SO + K - 1 staged rows along the axis of 64
+// columns; thread (cp, og) sums the column pair 2cp, 2cp+1 (packed FP32
+// pairs) for the 8 outputs 8og .. 8og+7 from a sliding window of 8 rows,
+// one new row per tap.
+__host__ __device__ constexpr int s_rows(int K) { return SO + K - 1; }
+
 template <class Tin, class Tout>
-__global__ void __launch_bounds__(NT) k_tpass_s(const __grid_constant__ TiledPassParams p)
+__global__ void __launch_bounds__(NT, 5) k_tpass_s(const __grid_constant__ TiledPassParams p)
 {
     extern __shared__ __align__(16) float sm_s[];
     const int K = p.ntap;
-    const int nr = SO + K - 1;                       // staged rows along the axis
-    float* s_w = sm_s + nr * SC;
+    const int nr = s_rows(K);
+    float2* s_w2 = reinterpret_cast<float2*>(sm_s + nr * SC);     // (w, w) pairs
     const int tid = threadIdx.x;
     const int a = p.axis;
     const int64_t n0 = p.n[0], na = p.n[a];
@@ -139,66 +215,101 @@ __global__ void __launch_bounds__(NT) k_tpass_s(const __grid_constant__ TiledPas
     int64_t so = 0, dof = 0;
     outer_offsets(p, 0, a, blockIdx.y, &so, &dof);
     const Tin* src = reinterpret_cast<const Tin*>(p.src) + so;
-    for (int i = tid; i < K; i += NT) s_w[i] = p.w[i];
+    for (int i = tid; i < ((K + 1) & ~1); i += NT) s_w2[i] = i < K ? make_float2(p.w[i], p.w[i]) : make_float2(0.f, 0.f);
     // staged rows r = 0 .. nr-1: axis coordinate y0 + omin + r, border-mapped;
     // columns x0 .. x0+63 (past n0: zero, never stored)
-    // rows of 64 columns inside the image, 16-byte aligned f32: float4 loads
+    const int64_t ys = y0 + p.omin;
+    const bool rows_in = ys >= 0 && ys + nr <= na;
     bool vec = false;
     if constexpr (sizeof(Tin) == 4)
         vec = p.ss[0] == 1 && x0 + SC <= n0 && (p.ss[a] & 3) == 0 && (reinterpret_cast<uintptr_t>(src + x0) & 15) == 0;
     if (vec) {
+        // a thread keeps one 16-byte column chunk, rows tid/16 + 16i
+        const int c4 = tid & 15;
+        const float* sp = reinterpret_cast<const float*>(src) + x0 + 4 * c4;
+        if (rows_in) {
+            const int64_t step = (NT / 16) * p.ss[a];
+            const float* g = sp + (ys + (tid >> 4)) * p.ss[a];
 #pragma unroll 4
-        for (int i = tid; i < nr * (SC / 4); i += NT) {
-            const int r = i / (SC / 4), c4 = i - (i / (SC / 4)) * (SC / 4);
-            int64_t y = y0 + p.omin + r;
-            if (y < 0 || y >= na) y = (y >= na + p.omax || y < p.omin) ? na - 1 : bmap(p.border, na, y);
-            *reinterpret_cast<float4*>(sm_s + r * SC + 4 * c4) =
-                *reinterpret_cast<const float4*>(src + x0 + 4 * c4 + y * p.ss[a]);
+            for (int r = tid >> 4; r < nr; r += NT / 16, g += step)
+                *reinterpret_cast<float4*>(sm_s + r * SC + 4 * c4) = *reinterpret_cast<const float4*>(g);
+        } else {
+#pragma unroll 4
+            for (int r = tid >> 4; r < nr; r += NT / 16) {
+                int64_t y = ys + r;
+                if (y < 0 || y >= na) y = (y >= na + p.omax || y < p.omin) ? na - 1 : bmap(p.border, na, y);
+                *reinterpret_cast<float4*>(sm_s + r * SC + 4 * c4) = *reinterpret_cast<const float4*>(sp + y * p.ss[a]);
+            }
         }
-    } else
-    // (unrolled so that the loads of several iterations are in flight at once)
-#pragma unroll 8
-    for (int i = tid; i < nr * SC; i += NT) {
-        const int r = i / SC, c = i - (i / SC) * SC;
-        float v = 0.f;
+    } else {
+        const int c = tid & (SC - 1);
         const int64_t x = x0 + c;
-        if (x < n0) {
-            int64_t y = y0 + p.omin + r;
-            if (y < 0 || y >= na) y = (y >= na + p.omax || y < p.omin) ? na - 1 : bmap(p.border, na, y);
-            v = ldf<Tin>(src + x * p.ss[0] + y * p.ss[a]);
+        const Tin* sp = src + x * p.ss[0];
+#pragma unroll 4
+        for (int r = tid / SC; r < nr; r += NT / SC) {
+            float v = 0.f;
+            if (x < n0) {
+                int64_t y = ys + r;
+                if (y < 0 || y >= na) y = (y >= na + p.omax || y < p.omin) ? na - 1 : bmap(p.border, na, y);
+                v = ldf<Tin>(sp + y * p.ss[a]);
+            }
+            sm_s[r * SC + c] = v;
         }
-        sm_s[i] = v;
     }
     __syncthreads();
     const int cp = tid & 31, og = tid >> 5;
-    float2 acc[4] = {make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
-    const float* col = sm_s + (4 * og) * SC + 2 * cp;
-    const int K4 = K & ~3;
-    for (int t = 0; t < K4; t += 4) {
-        float2 rows[7];
+    const float* col = sm_s + (8 * og) * SC + 2 * cp;
+    float2 acc[8], win[8];
 #pragma unroll
-        for (int j = 0; j < 7; j++) rows[j] = *reinterpret_cast<const float2*>(col + (t + j) * SC);
-        const float4 w = *reinterpret_cast<const float4*>(s_w + t);
-        const float wq[4] = {w.x, w.y, w.z, w.w};
+    for (int j = 0; j < 8; j++) acc[j] = make_float2(0.f, 0.f);
 #pragma unroll
-        for (int q = 0; q < 4; q++)
+    for (int j = 0; j < 7; j++) win[j] = *reinterpret_cast<const float2*>(col + j * SC);
+    const int K8 = K & ~7;
+    for (int t0 = 0; t0 < K8; t0 += 8) {
 #pragma unroll
-            for (int j = 0; j < 4; j++) acc[j] = __ffma2_rn(rows[j + q], make_float2(wq[q], wq[q]), acc[j]);
+        for (int u = 0; u < 8; u += 2) {
+            const float4 w = *reinterpret_cast<const float4*>(s_w2 + t0 + u);     // taps t0+u, t0+u+1
+            win[(u + 7) & 7] = *reinterpret_cast<const float2*>(col + (t0 + u + 7) * SC);
+#pragma unroll
+            for (int j = 0; j < 8; j++) acc[j] = __ffma2_rn(win[(u + j) & 7], make_float2(w.x, w.y), acc[j]);
+            win[(u + 8) & 7] = *reinterpret_cast<const float2*>(col + (t0 + u + 8) * SC);
+#pragma unroll
+            for (int j = 0; j < 8; j++) acc[j] = __ffma2_rn(win[(u + 1 + j) & 7], make_float2(w.z, w.w), acc[j]);
+        }
     }
-    for (int t = K4; t < K; t++) {
-        const float w = s_w[t];
+    // the last K mod 8 taps (t0 = K8, a multiple of 8: the same slots)
 #pragma unroll
-        for (int j = 0; j < 4; j++)
-            acc[j] = __ffma2_rn(*reinterpret_cast<const float2*>(col + (t + j) * SC), make_float2(w, w), acc[j]);
+    for (int u = 0; u < 7; u++) {
+        if (K8 + u >= K) break;
+        win[(u + 7) & 7] = *reinterpret_cast<const float2*>(col + (K8 + u + 7) * SC);
+        const float2 w = s_w2[K8 + u];
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[j] = __ffma2_rn(win[(u + j) & 7], w, acc[j]);
     }
     Tout* dst = reinterpret_cast<Tout*>(p.dst) + dof;
+    const int64_t xa = x0 + 2 * cp;
+    const int64_t ya = y0 + 8 * og;
+    const int nj = na - ya < 8 ? (int)(na - ya) : 8;
+    if (nj <= 0) return;
+    bool vst = false;
+    if constexpr (sizeof(Tout) == 4)
+        vst = p.ds[0] == 1 && (p.ds[a] & 1) == 0 && (reinterpret_cast<uintptr_t>(dst + x0) & 7) == 0 && xa + 2 <= n0;
+    Tout* d = dst + xa * p.ds[0] + ya * p.ds[a];
+    const int64_t dsa = p.ds[a];
+    if constexpr (sizeof(Tout) == 4) {
+        if (vst) {
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
-        const int64_t y = y0 + 4 * og + j;
-        if (y >= na) continue;
-        const int64_t xa = x0 + 2 * cp;
-        if (xa < n0) dst[xa * p.ds[0] + y * p.ds[a]] = stf<Tout>(acc[j].x);
-        if (xa + 1 < n0) dst[(xa + 1) * p.ds[0] + y * p.ds[a]] = stf<Tout>(acc[j].y);
+            for (int j = 0; j < 8; j++)
+                if (j < nj) *reinterpret_cast<float2*>(reinterpret_cast<float*>(d) + j * dsa) = acc[j];
+            return;
+        }
+    }
+    const int64_t ds0 = p.ds[0];
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        if (j >= nj) break;
+        if (xa < n0) d[j * dsa] = stf<Tout>(acc[j].x);
+        if (xa + 1 < n0) d[j * dsa + ds0] = stf<Tout>(acc[j].y);
     }
 }
 
@@ -210,8 +321,7 @@ cudaError_t launch_t(const TiledPassParams& p_in, cudaStream_t s)
     p.dtx.init((uint32_t)((p.n[0] + (p.axis == 0 ? XO : SC) - 1) / (p.axis == 0 ? XO : SC)));
     const int K = p.ntap;
     if (p.axis == 0) {
-        const int pitch = (XO + K + 3 + 3) & ~3;
-        const size_t smem = ((size_t)XR * pitch + ((K + 3) & ~3)) * sizeof(float);
+        const size_t smem = ((size_t)XR * x_pitch(K) + ((K + 3) & ~3)) * sizeof(float);
         const int64_t ntx = (p.n[0] + XO - 1) / XO;
         const int64_t nb = ntx * ((p.rows + XR - 1) / XR);
         if (nb > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
@@ -222,7 +332,7 @@ cudaError_t launch_t(const TiledPassParams& p_in, cudaStream_t s)
         }
         k_tpass_x<Tin, Tout><<<(unsigned)nb, NT, smem, s>>>(p);
     } else {
-        const size_t smem = ((size_t)(SO + K - 1) * SC + ((K + 3) & ~3)) * sizeof(float);
+        const size_t smem = (size_t)s_rows(K) * SC * sizeof(float) + (size_t)((K + 1) & ~1) * sizeof(float2);
         const int64_t ntx = (p.n[0] + SC - 1) / SC, nta = (p.n[p.axis] + SO - 1) / SO;
         const int64_t outer = p.rows / p.n[p.axis];
         if (ntx * nta > 0x7fffffffLL || outer > 65535) return cudaErrorInvalidConfiguration;
@@ -258,13 +368,13 @@ bool tiled_pass_supported(const TiledPassParams& p)
     if (p.ntap < 1 || p.ntap > kMaxTaps || p.omax - p.omin + 1 != p.ntap) return false;
     if (p.rows < 1 || p.rows >= (1LL << 31)) return false;
     for (int i = 0; i < p.rank; i++)
-        if (p.n[i] >= (1LL << 31)) return false;
-    // tiles of 128 (x pass) or 64 (other axes) contiguous columns: short x
+        if (p.n[i] >= (1LL << 30)) return false;
+    // tiles of 256 (x pass) or 64 (other axes) contiguous columns: short x
     // extents (a channel axis) keep the general kernel
     if (p.n[0] < (p.axis == 0 ? 16 : 32)) return false;
     // the staged window of the widest kernel must fit one CTA's shared memory
-    const size_t smx = ((size_t)XR * ((XO + p.ntap + 6) & ~3) + p.ntap + 3) * 4;
-    const size_t sms = ((size_t)(SO + p.ntap - 1) * SC + p.ntap + 3) * 4;
+    const size_t smx = ((size_t)XR * x_pitch(p.ntap) + p.ntap + 3) * 4;
+    const size_t sms = (size_t)s_rows(p.ntap) * SC * 4 + (size_t)(p.ntap + 1) * 8;
     if (smx > 200 * 1024 || sms > 200 * 1024) return false;
     if (p.axis != 0 && p.rows / p.n[p.axis] > 65535) return false;
     return true;
