@@ -15,13 +15,16 @@
 //   X pass: 4 columns x 1 row pair per thread, the same packed arithmetic
 //           (a word is the row pair of one column, so every tap reads an
 //           aligned word).
-//   Z pass: the X-pass values unpacked into a KZ-deep register queue (the
-//           slot of the newest plane rotates; compile-time slot dispatch),
-//           32-bit integer sums.
+//   Z pass: the X-pass row pairs as packed FP32 pairs of integers in a
+//           KZ-deep register queue (the slot of the newest plane rotates;
+//           compile-time slot dispatch), packed FP32 multiply-adds (every
+//           sum an integer below 2^23, exact), starting from the rounding's
+//           half unit.
 //   store : round (or truncate) the numerator once, as the reference's
-//           double result would be, and stage the bytes in shared memory so
-//           that 16-byte stores run along the destination's contiguous axis
-//           (X, or Y for a transposed destination).
+//           double result would be (one FP32 multiply-add rounded down onto
+//           the integer grid of [2^23, 2^24)), and stage the bytes in shared
+//           memory so that 16-byte stores run along the destination's
+//           contiguous axis (X, or Y for a transposed destination).
 // The packed lanes hold the Y sums and the X-of-Y sums, both below 2^16 by
 // the host's bound; the taps are non-negative.  Border maps are Clamp / Wrap
 // / Reflect of mathHelpers.h:23-25 on load coordinates only.
@@ -66,36 +69,48 @@ struct GU8 {
 __device__ __forceinline__ unsigned lo16(unsigned w) { return __byte_perm(w, 0u, 0x4140); }
 __device__ __forceinline__ unsigned hi16(unsigned w) { return __byte_perm(w, 0u, 0x4342); }
 
-// The Z queue: q[s][e] holds the X-pass value e (columns 4g + e/2, row 2rp +
-// e%2) of the plane in slot s; the newest plane is in slot S and tap k reads
-// slot (S + 1 + k) % KZ.
+// The Z queue: q[s][m] holds the X-pass values of column 4g + m, rows 2rp
+// and 2rp+1 (a packed FP32 pair), of the plane in slot s; the newest plane is
+// in slot S and tap k reads slot (S + 1 + k) % KZ.  The values and every Z
+// sum are integers below 2^23 (the host's bound), exact in FP32; the taps are
+// the integer numerators as FP32 pairs (wz2).
+// The sums start from a0 (the rounding's half unit, an integer).
 template <int KZ, int S>
-__device__ __forceinline__ void zstep_u8(unsigned (&q)[KZ][8], const unsigned (&xv)[8], unsigned (&o)[8],
-                                         const FusedParams& p)
+__device__ __forceinline__ void zstep_u8(float2 (&q)[KZ][4], const float2 (&xv)[4], float2 (&o)[4],
+                                         const FusedParams& p, float2 a0)
 {
 #pragma unroll
-    for (int e = 0; e < 8; e++) q[S][e] = xv[e];
+    for (int m = 0; m < 4; m++) q[S][m] = xv[m];
 #pragma unroll
-    for (int e = 0; e < 8; e++) {
-        unsigned a = 0;
+    for (int m = 0; m < 4; m++) {
+        float2 a = a0;
 #pragma unroll
-        for (int k = 0; k < KZ; k++) a += q[(S + 1 + k) % KZ][e] * (unsigned)p.wzi[k];
-        o[e] = a;
+        for (int k = 0; k < KZ; k++) a = __ffma2_rn(q[(S + 1 + k) % KZ][m], p.wz2[k], a);
+        o[m] = a;
     }
 }
 
 template <int KZ>
-__device__ __forceinline__ void zdispatch_u8(int slot, unsigned (&q)[KZ][8], const unsigned (&xv)[8],
-                                             unsigned (&o)[8], const FusedParams& p)
+__device__ __forceinline__ void zdispatch_u8(int slot, float2 (&q)[KZ][4], const float2 (&xv)[4], float2 (&o)[4],
+                                             const FusedParams& p, float2 a0)
 {
 #define NDLGPU_ZU8(S) \
-    case S: if constexpr (S < KZ) zstep_u8<KZ, (S < KZ ? S : 0)>(q, xv, o, p); break;
+    case S: if constexpr (S < KZ) zstep_u8<KZ, (S < KZ ? S : 0)>(q, xv, o, p, a0); break;
     switch (slot) {
         NDLGPU_ZU8(0) NDLGPU_ZU8(1) NDLGPU_ZU8(2) NDLGPU_ZU8(3) NDLGPU_ZU8(4) NDLGPU_ZU8(5) NDLGPU_ZU8(6)
         NDLGPU_ZU8(7) NDLGPU_ZU8(8)
     default: break;
     }
 #undef NDLGPU_ZU8
+}
+
+// A packed 16-bit lane as an FP32 integer: exponent bits of 2^23 over the
+// lane, minus 2^23 (exact).
+__device__ __forceinline__ float2 lanes_to_f2(unsigned w)
+{
+    const float2 b = make_float2(__uint_as_float(__byte_perm(w, 0x4B000000u, 0x7610)),
+                                 __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7632)));
+    return __fadd2_rn(b, make_float2(-8388608.f, -8388608.f));
 }
 
 template <int KX, int KY, int KZ, bool TS>
@@ -208,15 +223,21 @@ __global__ void __launch_bounds__(NT, 2) k_fused_u8(const __grid_constant__ Fuse
     // (a warp holds 16 row pairs x 2 column groups: the X-pass window loads
     // and the staged byte stores then fall on distinct banks)
     const int rp = tid & 15, g = tid >> 4;
-    unsigned q[KZ][8];
+    float2 q[KZ][4];
 #pragma unroll
     for (int s = 0; s < KZ; s++)
 #pragma unroll
-        for (int e = 0; e < 8; e++) q[s][e] = 0u;
+        for (int m = 0; m < 4; m++) q[s][m] = make_float2(0.f, 0.f);
     int slot = 0;
     int stage = 0, stage_next = STAGES - 1;
-    const int half = p.store_mode == STORE_ROUND && p.shift > 0 ? 1 << (p.shift - 1) : 0;
-    const int shift = p.shift;
+    // one rounding of the numerator S: floor((S + h) / 2^shift), h = 2^(shift-1)
+    // (round) or 0 (truncate).  The Z sums start from h, and the FP32
+    // multiply-add (S + h) * 2^-shift + 2^23 rounded down lands on the integer
+    // grid of [2^23, 2^24): the low byte of its bits is the result byte.
+    const float rscale = __uint_as_float((unsigned)(127 - p.shift) << 23);
+    const float rhalf = p.store_mode == STORE_ROUND && p.shift > 0 ? (float)(1 << (p.shift - 1)) : 0.f;
+    const float2 rscale2 = make_float2(rscale, rscale), rbias2 = make_float2(8388608.f, 8388608.f);
+    const float2 zinit = make_float2(rhalf, rhalf);
     // the Y pass: unit tid, and units 256..287 on the last warp
     const int nyu = tid >= NT - (NYU - NT) ? 2 : 1;
 
@@ -262,7 +283,7 @@ __global__ void __launch_bounds__(NT, 2) k_fused_u8(const __grid_constant__ Fuse
 
         // X pass: columns 4g .. 4g+3 of row pair rp; window of Y-pass words
         // 4g .. 4g+11 (columns x0-4+4g ..)
-        unsigned xv[8];
+        float2 xv[4];
         {
             const unsigned* wr = s_y + rp * YP + 4 * g;
             unsigned win[12];
@@ -276,28 +297,32 @@ __global__ void __launch_bounds__(NT, 2) k_fused_u8(const __grid_constant__ Fuse
                 unsigned a = 0;
 #pragma unroll
                 for (int k = 0; k < KX; k++) a += win[m + 4 - CX + k] * (unsigned)p.wxi[k];
-                xv[2 * m] = a & 0xffffu;
-                xv[2 * m + 1] = a >> 16;
+                xv[m] = lanes_to_f2(a);
             }
         }
-        unsigned o[8];
-        zdispatch_u8<KZ>(slot, q, xv, o, p);
+        float2 o[4];
+        zdispatch_u8<KZ>(slot, q, xv, o, p, zinit);
         slot = (slot + 1 == KZ) ? 0 : slot + 1;
         if (n >= KZ - 1) {
-            // one rounding of the numerator, then the byte
+            unsigned ob[4][2];   // column m: rows 2rp, 2rp+1; the result in the low byte
 #pragma unroll
-            for (int e = 0; e < 8; e++) o[e] = ((o[e] + (unsigned)half) >> shift) & 0xffu;
+            for (int m = 0; m < 4; m++) {
+                const float2 r = __ffma2_rd(o[m], rscale2, rbias2);
+                ob[m][0] = __float_as_uint(r.x);
+                ob[m][1] = __float_as_uint(r.y);
+            }
             if constexpr (TS) {
                 // staged x-major: the destination is contiguous along Y
 #pragma unroll
                 for (int m = 0; m < 4; m++) {
-                    const unsigned short v2 = (unsigned short)(o[2 * m] | (o[2 * m + 1] << 8));
+                    const unsigned short v2 = (unsigned short)__byte_perm(ob[m][0], ob[m][1], 0x0040);
                     *reinterpret_cast<unsigned short*>(s_o + (4 * g + m) * TY + 2 * rp) = v2;
                 }
             } else {
 #pragma unroll
                 for (int h = 0; h < 2; h++) {
-                    const unsigned v4 = o[h] | (o[2 + h] << 8) | (o[4 + h] << 16) | (o[6 + h] << 24);
+                    const unsigned v4 = __byte_perm(__byte_perm(ob[0][h], ob[1][h], 0x0040),
+                                                    __byte_perm(ob[2][h], ob[3][h], 0x0040), 0x5410);
                     *reinterpret_cast<unsigned*>(s_o + (2 * rp + h) * (TX + 4) + 4 * g) = v4;
                 }
             }
@@ -352,6 +377,11 @@ cudaError_t launch_u8(const FusedParams& p_in, cudaStream_t s)
     static_assert(G::SMEM <= 113 * 1024, "two CTAs per SM");
     static bool configured[2] = {false, false};
     FusedParams p = p_in;
+    // the Z taps' integer numerators as FP32 pairs (exact below 2^24)
+    for (int k = 0; k < 40; k++) {
+        const float w = k < p.kz ? (float)p.wzi[k] : 0.f;
+        p.wz2[k] = make_float2(w, w);
+    }
     // 16-byte stores along Y for a transposed destination, 4-byte ones along X
     // otherwise
     const auto al16 = [](int64_t v) { return v % 16 == 0; };
@@ -418,10 +448,11 @@ bool fused_u8_supported(const FusedParams& p)
     for (int k = 0; k < p.ky; k++) if (p.wyi[k] < 0) return false;
     for (int k = 0; k < p.kz; k++) if (p.wzi[k] < 0) return false;
     // packed lanes: the Y sums and the X-of-Y sums of bytes stay below 2^16;
-    // the Z sums in 32 bits
+    // the Z sums plus the rounding's half unit (FP32 integers) below 2^23
     const long long sy = tap_sum(p.wyi, p.ky), sx = tap_sum(p.wxi, p.kx), sz = tap_sum(p.wzi, p.kz);
     if (255 * sy >= 65536 || 255 * sy * sx >= 65536) return false;
-    if (255 * sy * sx * sz >= (1LL << 31)) return false;
+    const long long half = p.shift > 0 ? 1LL << (p.shift - 1) : 0;
+    if (255 * sy * sx * sz + half >= (1LL << 23)) return false;
     return true;
 }
 
