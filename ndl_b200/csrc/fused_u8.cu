@@ -41,7 +41,6 @@ constexpr int RP = 96;           // ring row: bytes x0-16 .. x0+79 (6 chunks)
 constexpr int NCH = RP / 16;
 constexpr int YW = 18;           // Y-pass words per row pair: columns x0-4 .. x0+67
 constexpr int YP = 4 * YW + 4;   // ... row-pair pitch in words (+ a bank shift)
-constexpr int NYU = YW * TY / 2; // Y-pass units (288)
 
 __device__ __forceinline__ void cp_async16(unsigned saddr, const void* gmem)
 {
@@ -238,8 +237,6 @@ __global__ void __launch_bounds__(NT, 2) k_fused_u8(const __grid_constant__ Fuse
     const float rhalf = p.store_mode == STORE_ROUND && p.shift > 0 ? (float)(1 << (p.shift - 1)) : 0.f;
     const float2 rscale2 = make_float2(rscale, rscale), rbias2 = make_float2(8388608.f, 8388608.f);
     const float2 zinit = make_float2(rhalf, rhalf);
-    // the Y pass: unit tid, and units 256..287 on the last warp
-    const int nyu = tid >= NT - (NYU - NT) ? 2 : 1;
 
     for (int n = 0; n < nplanes; n++) {
         cp_async_wait<STAGES - 2>();
@@ -252,10 +249,13 @@ __global__ void __launch_bounds__(NT, 2) k_fused_u8(const __grid_constant__ Fuse
         const unsigned char* sb = s_in + stage * G::STAGE;
         stage = (stage + 1 == STAGES) ? 0 : stage + 1;
 
-        // Y pass: word w (columns x0-4+4w ..), rows 2yp, 2yp+1
-        for (int v = 0; v < nyu; v++) {
-            const int u = v == 0 ? tid : tid + (NYU - NT);
-            const int yp = u / YW, w = u - (u / YW) * YW;
+        // Y pass: word w (columns x0-4+4w ..), rows 2yp, 2yp+1.  Thread tid
+        // takes the inner word 1 + (tid & 15) of row pair tid >> 4 (a warp
+        // reads two row pairs' 64 inner bytes: no bank conflict); the last
+        // warp also takes the two halo words of every row pair as half units
+        // (the two columns of each that the X pass reads).
+        {
+            const int yp = tid >> 4, w = 1 + (tid & 15);
             const unsigned char* col = sb + (2 * yp) * RP + 12 + 4 * w;
             unsigned a0l = 0, a0h = 0, a1l = 0, a1h = 0;   // rows 2yp / 2yp+1, columns (0,1) / (2,3)
 #pragma unroll
@@ -278,6 +278,24 @@ __global__ void __launch_bounds__(NT, 2) k_fused_u8(const __grid_constant__ Fuse
             o.z = __byte_perm(a0h, a1h, 0x5410);
             o.w = __byte_perm(a0h, a1h, 0x7632);
             *reinterpret_cast<uint4*>(s_y + yp * YP + 4 * w) = o;
+        }
+        if (tid >= NT - 32) {
+            // halo unit h: row pair h >> 1; word 0 (columns x0-2, x0-1: the
+            // high lanes) or word YW-1 (columns x0+64, x0+65: the low lanes)
+            const int h = tid - (NT - 32), yp = h >> 1;
+            const bool right = (h & 1) != 0;
+            const int w = right ? YW - 1 : 0;
+            const unsigned sel = right ? 0x4140u : 0x4342u;
+            const unsigned char* col = sb + (2 * yp) * RP + 12 + 4 * w;
+            unsigned a0 = 0, a1 = 0;
+#pragma unroll
+            for (int j = 0; j < KY + 1; j++) {
+                const unsigned lane = __byte_perm(*reinterpret_cast<const unsigned*>(col + j * RP), 0u, sel);
+                if (j < KY) a0 += lane * (unsigned)p.wyi[j];
+                if (j >= 1) a1 += lane * (unsigned)p.wyi[j - 1];
+            }
+            *reinterpret_cast<uint2*>(s_y + yp * YP + 4 * w + (right ? 0 : 2)) =
+                make_uint2(__byte_perm(a0, a1, 0x5410), __byte_perm(a0, a1, 0x7632));
         }
         __syncthreads();
 
