@@ -112,8 +112,9 @@ struct TiledPassParams {
     int ntap, omin, omax;
     int64_t rows;                 // product of the extents of every axis but 0
     int64_t n[kTiledRank], ss[kTiledRank], ds[kTiledRank];
-    FastDiv dv[kTiledRank];       // dividers of the extents, and of the tile count along x
-    FastDiv dtx;
+    FastDiv dv[kTiledRank];       // dividers of the extents, of the tile count along x,
+    FastDiv dtx;                  // and (strided pass) of the tile count along the axis
+    FastDiv dta;
     float w[kMaxTaps];
 };
 bool tiled_pass_supported(const TiledPassParams& p);

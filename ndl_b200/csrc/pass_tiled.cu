@@ -15,6 +15,8 @@
 //     pair (packed FP32 pairs) and 8 outputs along the axis, one new row per
 //     tap.
 // Taps are the pass's dense offsets omin .. omin+K-1 in ascending order.
+#include <algorithm>
+
 #include "dtype.cuh"
 
 namespace ndlgpu {
@@ -197,53 +199,63 @@ __global__ void __launch_bounds__(NT) k_tpass_x(const __grid_constant__ TiledPas
 // Strided pass (any axis but x): SO + K - 1 staged rows along the axis of 64
 // columns; thread (cp, og) sums the column pair 2cp, 2cp+1 (packed FP32
 // pairs) for the 8 outputs 8og .. 8og+7 from a sliding window of 8 rows,
-// one new row per tap.
+// one new row per tap.  Persistent CTAs walk the tiles with two staging
+// buffers: the rows of the next tile load (cp.async, 16-byte chunks) while
+// the current one is summed.
 __host__ __device__ constexpr int s_rows(int K) { return SO + K - 1; }
 
-template <class Tin, class Tout>
-__global__ void __launch_bounds__(NT, 5) k_tpass_s(const __grid_constant__ TiledPassParams p)
+__device__ __forceinline__ void cp_async16(float* smem, const float* gmem)
 {
-    extern __shared__ __align__(16) float sm_s[];
-    const int K = p.ntap;
-    const int nr = s_rows(K);
-    float2* s_w2 = reinterpret_cast<float2*>(sm_s + nr * SC);     // (w, w) pairs
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+struct STile {
+    int64_t x0, y0, so, dof;
+};
+
+__device__ __forceinline__ STile s_tile(const TiledPassParams& p, uint32_t t)
+{
+    STile r;
+    const uint32_t q = p.dtx.div(t), tx = t - q * p.dtx.d;
+    const uint32_t o = p.dta.div(q), ta = q - o * p.dta.d;
+    r.x0 = (int64_t)tx * SC;
+    r.y0 = (int64_t)ta * SO;
+    outer_offsets(p, 0, p.axis, o, &r.so, &r.dof);
+    return r;
+}
+
+// Rows r = 0 .. nr-1 of a tile into buf: axis coordinate y0 + omin + r,
+// border-mapped; columns x0 .. x0+63 (past n0: zero, never stored).  Whole
+// 16-byte chunks of contiguous f32 rows go by cp.async, the rest by loads.
+template <class Tin>
+__device__ __forceinline__ void s_stage(const TiledPassParams& p, const STile& tl, float* buf, int nr)
+{
     const int tid = threadIdx.x;
     const int a = p.axis;
     const int64_t n0 = p.n[0], na = p.n[a];
-    const uint32_t ta = p.dtx.div(blockIdx.x), tx = blockIdx.x - ta * p.dtx.d;
-    const int64_t x0 = (int64_t)tx * SC, y0 = (int64_t)ta * SO;
-    int64_t so = 0, dof = 0;
-    outer_offsets(p, 0, a, blockIdx.y, &so, &dof);
-    const Tin* src = reinterpret_cast<const Tin*>(p.src) + so;
-    for (int i = tid; i < ((K + 1) & ~1); i += NT) s_w2[i] = i < K ? make_float2(p.w[i], p.w[i]) : make_float2(0.f, 0.f);
-    // staged rows r = 0 .. nr-1: axis coordinate y0 + omin + r, border-mapped;
-    // columns x0 .. x0+63 (past n0: zero, never stored)
-    const int64_t ys = y0 + p.omin;
-    const bool rows_in = ys >= 0 && ys + nr <= na;
+    const Tin* src = reinterpret_cast<const Tin*>(p.src) + tl.so;
+    const int64_t ys = tl.y0 + p.omin;
     bool vec = false;
     if constexpr (sizeof(Tin) == 4)
-        vec = p.ss[0] == 1 && x0 + SC <= n0 && (p.ss[a] & 3) == 0 && (reinterpret_cast<uintptr_t>(src + x0) & 15) == 0;
+        vec = p.ss[0] == 1 && tl.x0 + SC <= n0 && (p.ss[a] & 3) == 0 &&
+              (reinterpret_cast<uintptr_t>(src + tl.x0) & 15) == 0;
     if (vec) {
         // a thread keeps one 16-byte column chunk, rows tid/16 + 16i
         const int c4 = tid & 15;
-        const float* sp = reinterpret_cast<const float*>(src) + x0 + 4 * c4;
-        if (rows_in) {
-            const int64_t step = (NT / 16) * p.ss[a];
-            const float* g = sp + (ys + (tid >> 4)) * p.ss[a];
+        const float* sp = reinterpret_cast<const float*>(src) + tl.x0 + 4 * c4;
 #pragma unroll 4
-            for (int r = tid >> 4; r < nr; r += NT / 16, g += step)
-                *reinterpret_cast<float4*>(sm_s + r * SC + 4 * c4) = *reinterpret_cast<const float4*>(g);
-        } else {
-#pragma unroll 4
-            for (int r = tid >> 4; r < nr; r += NT / 16) {
-                int64_t y = ys + r;
-                if (y < 0 || y >= na) y = (y >= na + p.omax || y < p.omin) ? na - 1 : bmap(p.border, na, y);
-                *reinterpret_cast<float4*>(sm_s + r * SC + 4 * c4) = *reinterpret_cast<const float4*>(sp + y * p.ss[a]);
-            }
+        for (int r = tid >> 4; r < nr; r += NT / 16) {
+            int64_t y = ys + r;
+            if (y < 0 || y >= na) y = (y >= na + p.omax || y < p.omin) ? na - 1 : bmap(p.border, na, y);
+            cp_async16(buf + r * SC + 4 * c4, sp + y * p.ss[a]);
         }
     } else {
         const int c = tid & (SC - 1);
-        const int64_t x = x0 + c;
+        const int64_t x = tl.x0 + c;
         const Tin* sp = src + x * p.ss[0];
 #pragma unroll 4
         for (int r = tid / SC; r < nr; r += NT / SC) {
@@ -253,12 +265,21 @@ __global__ void __launch_bounds__(NT, 5) k_tpass_s(const __grid_constant__ Tiled
                 if (y < 0 || y >= na) y = (y >= na + p.omax || y < p.omin) ? na - 1 : bmap(p.border, na, y);
                 v = ldf<Tin>(sp + y * p.ss[a]);
             }
-            sm_s[r * SC + c] = v;
+            buf[r * SC + c] = v;
         }
     }
-    __syncthreads();
+}
+
+template <class Tout>
+__device__ __forceinline__ void s_sum_store(const TiledPassParams& p, const STile& tl, const float* buf,
+                                            const float2* s_w2)
+{
+    const int K = p.ntap;
+    const int tid = threadIdx.x;
+    const int a = p.axis;
+    const int64_t n0 = p.n[0], na = p.n[a];
     const int cp = tid & 31, og = tid >> 5;
-    const float* col = sm_s + (8 * og) * SC + 2 * cp;
+    const float* col = buf + (8 * og) * SC + 2 * cp;
     float2 acc[8], win[8];
 #pragma unroll
     for (int j = 0; j < 8; j++) acc[j] = make_float2(0.f, 0.f);
@@ -286,14 +307,15 @@ __global__ void __launch_bounds__(NT, 5) k_tpass_s(const __grid_constant__ Tiled
 #pragma unroll
         for (int j = 0; j < 8; j++) acc[j] = __ffma2_rn(win[(u + j) & 7], w, acc[j]);
     }
-    Tout* dst = reinterpret_cast<Tout*>(p.dst) + dof;
-    const int64_t xa = x0 + 2 * cp;
-    const int64_t ya = y0 + 8 * og;
+    Tout* dst = reinterpret_cast<Tout*>(p.dst) + tl.dof;
+    const int64_t xa = tl.x0 + 2 * cp;
+    const int64_t ya = tl.y0 + 8 * og;
     const int nj = na - ya < 8 ? (int)(na - ya) : 8;
     if (nj <= 0) return;
     bool vst = false;
     if constexpr (sizeof(Tout) == 4)
-        vst = p.ds[0] == 1 && (p.ds[a] & 1) == 0 && (reinterpret_cast<uintptr_t>(dst + x0) & 7) == 0 && xa + 2 <= n0;
+        vst = p.ds[0] == 1 && (p.ds[a] & 1) == 0 && (reinterpret_cast<uintptr_t>(dst + tl.x0) & 7) == 0 &&
+              xa + 2 <= n0;
     Tout* d = dst + xa * p.ds[0] + ya * p.ds[a];
     const int64_t dsa = p.ds[a];
     if constexpr (sizeof(Tout) == 4) {
@@ -311,6 +333,40 @@ __global__ void __launch_bounds__(NT, 5) k_tpass_s(const __grid_constant__ Tiled
         if (xa < n0) d[j * dsa] = stf<Tout>(acc[j].x);
         if (xa + 1 < n0) d[j * dsa + ds0] = stf<Tout>(acc[j].y);
     }
+}
+
+template <class Tin, class Tout>
+__global__ void __launch_bounds__(NT, 4) k_tpass_s(const __grid_constant__ TiledPassParams p, uint32_t ntiles)
+{
+    extern __shared__ __align__(16) float sm_s[];
+    const int K = p.ntap;
+    const int nr = s_rows(K);
+    float2* s_w2 = reinterpret_cast<float2*>(sm_s + 2 * nr * SC);     // (w, w) pairs
+    const int tid = threadIdx.x;
+    for (int i = tid; i < ((K + 1) & ~1); i += NT) s_w2[i] = i < K ? make_float2(p.w[i], p.w[i]) : make_float2(0.f, 0.f);
+    uint32_t t = blockIdx.x;
+    if (t >= ntiles) return;
+    STile cur = s_tile(p, t);
+    s_stage<Tin>(p, cur, sm_s, nr);
+    cp_async_commit();
+    for (int i = 0; t < ntiles; i++) {
+        const uint32_t tn = t + gridDim.x;
+        STile nxt = cur;
+        if (tn < ntiles) {
+            // the buffer of tile i+1 was last read by tile i-1, before the
+            // barrier that ended its step
+            nxt = s_tile(p, tn);
+            s_stage<Tin>(p, nxt, sm_s + ((i + 1) & 1) * nr * SC, nr);
+        }
+        cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();   // tile i's rows (every thread's copies) and the taps visible
+        s_sum_store<Tout>(p, cur, sm_s + (i & 1) * nr * SC, s_w2);
+        __syncthreads();   // every thread is done with buffer i & 1
+        cur = nxt;
+        t = tn;
+    }
+    cp_async_wait<0>();
 }
 
 template <class Tin, class Tout>
@@ -332,16 +388,25 @@ cudaError_t launch_t(const TiledPassParams& p_in, cudaStream_t s)
         }
         k_tpass_x<Tin, Tout><<<(unsigned)nb, NT, smem, s>>>(p);
     } else {
-        const size_t smem = (size_t)s_rows(K) * SC * sizeof(float) + (size_t)((K + 1) & ~1) * sizeof(float2);
+        const size_t smem = 2 * (size_t)s_rows(K) * SC * sizeof(float) + (size_t)((K + 1) & ~1) * sizeof(float2);
         const int64_t ntx = (p.n[0] + SC - 1) / SC, nta = (p.n[p.axis] + SO - 1) / SO;
         const int64_t outer = p.rows / p.n[p.axis];
-        if (ntx * nta > 0x7fffffffLL || outer > 65535) return cudaErrorInvalidConfiguration;
+        const int64_t ntiles = ntx * nta * outer;
+        if (ntiles > 0x7fffffffLL || ntx * nta > 0xffffffffLL) return cudaErrorInvalidConfiguration;
+        p.dta.init((uint32_t)nta);
+        auto kern = k_tpass_s<Tin, Tout>;
         if (smem > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(k_tpass_s<Tin, Tout>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)smem);
+            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return e;
         }
-        k_tpass_s<Tin, Tout><<<dim3((unsigned)(ntx * nta), (unsigned)outer), NT, smem, s>>>(p);
+        // persistent CTAs: as many as fit at once
+        int dev = 0, sms = 148, per_sm = 1;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem);
+        if (per_sm < 1) per_sm = 1;
+        const int64_t grid = std::min<int64_t>(ntiles, (int64_t)sms * per_sm);
+        kern<<<(unsigned)grid, NT, smem, s>>>(p, (uint32_t)ntiles);
     }
     count_launch();
     return cudaGetLastError();
@@ -374,9 +439,8 @@ bool tiled_pass_supported(const TiledPassParams& p)
     if (p.n[0] < (p.axis == 0 ? 16 : 32)) return false;
     // the staged window of the widest kernel must fit one CTA's shared memory
     const size_t smx = ((size_t)XR * x_pitch(p.ntap) + p.ntap + 3) * 4;
-    const size_t sms = (size_t)s_rows(p.ntap) * SC * 4 + (size_t)(p.ntap + 1) * 8;
+    const size_t sms = 2 * (size_t)s_rows(p.ntap) * SC * 4 + (size_t)(p.ntap + 1) * 8;
     if (smx > 200 * 1024 || sms > 200 * 1024) return false;
-    if (p.axis != 0 && p.rows / p.n[p.axis] > 65535) return false;
     return true;
 }
 
