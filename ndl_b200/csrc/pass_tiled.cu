@@ -14,7 +14,10 @@
 //   along another axis: 64 columns x 64 outputs per CTA, a thread a column
 //     pair (packed FP32 pairs) and 8 outputs along the axis, one new row per
 //     tap.
-// Taps are the pass's dense offsets omin .. omin+K-1 in ascending order.
+// Both kernels are persistent: a CTA walks its tiles with two staging
+// buffers, cp.async loading the next tile's rows while the current one is
+// summed.  Taps are the pass's dense offsets omin .. omin+K-1 in ascending
+// order.
 #include <algorithm>
 
 #include "dtype.cuh"
@@ -58,6 +61,25 @@ __device__ __forceinline__ void outer_offsets(const TiledPassParams& p, int skip
     *dof = d;
 }
 
+__device__ __forceinline__ void cp_async16(float* smem, const float* gmem)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(float* smem, const float* gmem)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(float* smem, const float* gmem)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
 // x pass: the window of row `row` from x0 + omin, Lr floats (the outputs'
 // XO + K - 1 plus the chunk the last step reads past it), staged so that
 // srow[j] holds the input at x0 + omin + j.  Global reads are 16-byte chunks
@@ -91,68 +113,77 @@ __device__ __forceinline__ void taps_tail(float (&a)[4], const float4 A, const f
     }
 }
 
-template <class Tin, class Tout>
-__global__ void __launch_bounds__(NT) k_tpass_x(const __grid_constant__ TiledPassParams p)
+struct XTile {
+    uint32_t row;
+    int64_t x0, so, dof;
+};
+
+__device__ __forceinline__ XTile x_tile(const TiledPassParams& p, uint32_t t, int warp)
 {
-    extern __shared__ __align__(16) float sm_x[];
-    const int K = p.ntap;
-    const int L = x_window(K);
-    float* s_w = sm_x + XR * x_pitch(K);
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int64_t n0 = p.n[0];
-    const uint32_t rb = p.dtx.div(blockIdx.x), tx = blockIdx.x - rb * p.dtx.d;
-    const int64_t x0 = (int64_t)tx * XO;
-    const uint32_t nrows = (uint32_t)p.rows;
-    const int K4 = (K + 3) & ~3;
-    for (int i = tid; i < K4; i += NT) s_w[i] = i < K ? p.w[i] : 0.f;
-    const uint32_t row = rb * XR + warp;
-    int64_t so = 0, dof = 0;
-    if (row < nrows) outer_offsets(p, 0, -1, row, &so, &dof);
-    const Tin* src = reinterpret_cast<const Tin*>(p.src) + so;
-    float* srow = sm_x + warp * x_pitch(K) + 4;
-    if (row < nrows) {
-        // coordinates fit 32 bits (extents below 2^30)
-        const int n0i = (int)n0;
-        const int gs = (int)x0 + p.omin;
-        const int xs = gs & ~3;
-        const int rem = gs - xs;
-        const int nv = (L + rem + 3) >> 2;
-        // chunks va .. vb-1 lie wholly inside [0, n0) and load as float4
-        int va = 0, vb = 0;
-        if constexpr (sizeof(Tin) == 4) {
-            if (p.ss[0] == 1 && (reinterpret_cast<uintptr_t>(src) & 15) == 0) {
-                va = min(nv, xs >= 0 ? 0 : -xs >> 2);
-                vb = max(va, min(nv, (n0i - xs) >> 2));
-            }
-            const float* s4 = reinterpret_cast<const float*>(src) + xs;
-#pragma unroll 3
-            for (int v = va + lane; v < vb; v += 32) {
-                const float4 t = *reinterpret_cast<const float4*>(s4 + 4 * v);
-                float* d = srow + 4 * v - rem;
-                if (rem == 0) {
-                    *reinterpret_cast<float4*>(d) = t;
-                } else if (rem == 2) {
-                    *reinterpret_cast<float2*>(d) = make_float2(t.x, t.y);
-                    *reinterpret_cast<float2*>(d + 2) = make_float2(t.z, t.w);
-                } else {
-                    d[0] = t.x;
-                    *reinterpret_cast<float2*>(d + 1) = make_float2(t.y, t.z);
-                    d[3] = t.w;
-                }
-            }
+    XTile r;
+    const uint32_t rb = p.dtx.div(t), tx = t - rb * p.dtx.d;
+    r.x0 = (int64_t)tx * XO;
+    r.row = rb * XR + warp;
+    r.so = r.dof = 0;
+    if (r.row < (uint32_t)p.rows) outer_offsets(p, 0, -1, r.row, &r.so, &r.dof);
+    return r;
+}
+
+// The window of one row into srow (see x_window): whole 16-byte chunks of a
+// contiguous f32 row by cp.async (16, 8 or 4 bytes at a time, as the
+// window's offset rem into its first chunk allows), every other element by a
+// border-mapped load.
+template <class Tin>
+__device__ __forceinline__ void x_stage(const TiledPassParams& p, const XTile& tl, float* srow, int lane)
+{
+    if (tl.row >= (uint32_t)p.rows) return;
+    const int L = x_window(p.ntap);
+    const Tin* src = reinterpret_cast<const Tin*>(p.src) + tl.so;
+    // coordinates fit 32 bits (extents below 2^30)
+    const int n0i = (int)p.n[0];
+    const int gs = (int)tl.x0 + p.omin;
+    const int xs = gs & ~3;
+    const int rem = gs - xs;
+    const int nv = (L + rem + 3) >> 2;
+    // chunks va .. vb-1 lie wholly inside [0, n0)
+    int va = 0, vb = 0;
+    if constexpr (sizeof(Tin) == 4) {
+        if (p.ss[0] == 1 && (reinterpret_cast<uintptr_t>(src) & 15) == 0) {
+            va = min(nv, xs >= 0 ? 0 : -xs >> 2);
+            vb = max(va, min(nv, (n0i - xs) >> 2));
         }
-        // every other element of the window (the row's ends, or the whole
-        // window of a strided or 16-bit row): coordinates border-mapped
-        const int nlead = 4 * va, nrest = nlead + 4 * (nv - vb);
-        for (int i = lane; i < nrest; i += 32) {
-            const int e = i < nlead ? i : 4 * vb + (i - nlead);
-            int x = xs + e;
-            if (x < 0 || x >= n0i) x = (x >= n0i + p.omax || x < p.omin) ? n0i - 1 : map_border32(p.border, n0i, x);
-            srow[e - rem] = ldf<Tin>(src + (int64_t)x * p.ss[0]);
+        const float* s4 = reinterpret_cast<const float*>(src) + xs;
+#pragma unroll 3
+        for (int v = va + lane; v < vb; v += 32) {
+            const float* g = s4 + 4 * v;
+            float* d = srow + 4 * v - rem;
+            if (rem == 0) {
+                cp_async16(d, g);
+            } else if (rem == 2) {
+                cp_async8(d, g);
+                cp_async8(d + 2, g + 2);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 4; k++) cp_async4(d + k, g + k);
+            }
         }
     }
-    __syncthreads();
-    if (row >= nrows) return;
+    const int nlead = 4 * va, nrest = nlead + 4 * (nv - vb);
+    for (int i = lane; i < nrest; i += 32) {
+        const int e = i < nlead ? i : 4 * vb + (i - nlead);
+        int x = xs + e;
+        if (x < 0 || x >= n0i) x = (x >= n0i + p.omax || x < p.omin) ? n0i - 1 : map_border32(p.border, n0i, x);
+        srow[e - rem] = ldf<Tin>(src + (int64_t)x * p.ss[0]);
+    }
+}
+
+template <class Tout>
+__device__ __forceinline__ void x_sum_store(const TiledPassParams& p, const XTile& tl, const float* srow,
+                                            const float* s_w, int lane)
+{
+    if (tl.row >= (uint32_t)p.rows) return;
+    const int K = p.ntap;
+    const int64_t n0 = p.n[0];
     // lane l: outputs 4l .. 4l+3 and 128+4l .. 128+4l+3 (16-byte lane stride:
     // conflict-free window reads); a sliding window of two chunks per block
     const float* b0 = srow + 4 * lane;
@@ -177,13 +208,13 @@ __global__ void __launch_bounds__(NT) k_tpass_x(const __grid_constant__ TiledPas
         taps_tail(a0, A0, B0, w, K & 3);
         taps_tail(a1, A1, B1, w, K & 3);
     }
-    Tout* dst = reinterpret_cast<Tout*>(p.dst) + dof;
+    Tout* dst = reinterpret_cast<Tout*>(p.dst) + tl.dof;
     bool vst = false;
     if constexpr (sizeof(Tout) == 4) vst = p.ds[0] == 1 && (reinterpret_cast<uintptr_t>(dst) & 15) == 0;
 #pragma unroll
     for (int h = 0; h < 2; h++) {
         const float* a = h ? a1 : a0;
-        const int64_t xb = x0 + 4 * lane + h * (XO / 2);
+        const int64_t xb = tl.x0 + 4 * lane + h * (XO / 2);
         if constexpr (sizeof(Tout) == 4) {
             if (vst && xb + 4 <= n0) {
                 *reinterpret_cast<float4*>(reinterpret_cast<float*>(dst) + xb) = make_float4(a[0], a[1], a[2], a[3]);
@@ -196,6 +227,44 @@ __global__ void __launch_bounds__(NT) k_tpass_x(const __grid_constant__ TiledPas
     }
 }
 
+// Persistent CTAs walk the tiles (8 rows x 256 outputs) with two staging
+// buffers: the windows of the next tile load while the current one is summed.
+template <class Tin, class Tout>
+__global__ void __launch_bounds__(NT) k_tpass_x(const __grid_constant__ TiledPassParams p, uint32_t ntiles)
+{
+    extern __shared__ __align__(16) float sm_x[];
+    const int K = p.ntap;
+    const int P = x_pitch(K);
+    float* s_w = sm_x + 2 * XR * P;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int K4 = (K + 3) & ~3;
+    for (int i = tid; i < K4; i += NT) s_w[i] = i < K ? p.w[i] : 0.f;
+    uint32_t t = blockIdx.x;
+    if (t >= ntiles) return;
+    __syncthreads();   // the taps visible; from here each warp works on its own rows
+    XTile cur = x_tile(p, t, warp);
+    x_stage<Tin>(p, cur, sm_x + warp * P + 4, lane);
+    cp_async_commit();
+    for (int i = 0; t < ntiles; i++) {
+        const uint32_t tn = t + gridDim.x;
+        XTile nxt = cur;
+        if (tn < ntiles) {
+            // the warp's row of buffer i+1 was last read by tile i-1, before
+            // the warp barrier that ended its step
+            nxt = x_tile(p, tn, warp);
+            x_stage<Tin>(p, nxt, sm_x + (((i + 1) & 1) * XR + warp) * P + 4, lane);
+        }
+        cp_async_commit();
+        cp_async_wait<1>();
+        __syncwarp();   // tile i's window (every lane's copies) visible to the warp
+        x_sum_store<Tout>(p, cur, sm_x + ((i & 1) * XR + warp) * P + 4, s_w, lane);
+        __syncwarp();   // every lane is done with the warp's row of buffer i & 1
+        cur = nxt;
+        t = tn;
+    }
+    cp_async_wait<0>();
+}
+
 // Strided pass (any axis but x): SO + K - 1 staged rows along the axis of 64
 // columns; thread (cp, og) sums the column pair 2cp, 2cp+1 (packed FP32
 // pairs) for the 8 outputs 8og .. 8og+7 from a sliding window of 8 rows,
@@ -203,15 +272,6 @@ __global__ void __launch_bounds__(NT) k_tpass_x(const __grid_constant__ TiledPas
 // buffers: the rows of the next tile load (cp.async, 16-byte chunks) while
 // the current one is summed.
 __host__ __device__ constexpr int s_rows(int K) { return SO + K - 1; }
-
-__device__ __forceinline__ void cp_async16(float* smem, const float* gmem)
-{
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 struct STile {
     int64_t x0, y0, so, dof;
@@ -377,16 +437,23 @@ cudaError_t launch_t(const TiledPassParams& p_in, cudaStream_t s)
     p.dtx.init((uint32_t)((p.n[0] + (p.axis == 0 ? XO : SC) - 1) / (p.axis == 0 ? XO : SC)));
     const int K = p.ntap;
     if (p.axis == 0) {
-        const size_t smem = ((size_t)XR * x_pitch(K) + ((K + 3) & ~3)) * sizeof(float);
+        const size_t smem = (2 * (size_t)XR * x_pitch(K) + ((K + 3) & ~3)) * sizeof(float);
         const int64_t ntx = (p.n[0] + XO - 1) / XO;
-        const int64_t nb = ntx * ((p.rows + XR - 1) / XR);
-        if (nb > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+        const int64_t ntiles = ntx * ((p.rows + XR - 1) / XR);
+        if (ntiles > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+        auto kern = k_tpass_x<Tin, Tout>;
         if (smem > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(k_tpass_x<Tin, Tout>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)smem);
+            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return e;
         }
-        k_tpass_x<Tin, Tout><<<(unsigned)nb, NT, smem, s>>>(p);
+        // persistent CTAs: as many as fit at once
+        int dev = 0, sms = 148, per_sm = 1;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem);
+        if (per_sm < 1) per_sm = 1;
+        const int64_t grid = std::min<int64_t>(ntiles, (int64_t)sms * per_sm);
+        kern<<<(unsigned)grid, NT, smem, s>>>(p, (uint32_t)ntiles);
     } else {
         const size_t smem = 2 * (size_t)s_rows(K) * SC * sizeof(float) + (size_t)((K + 1) & ~1) * sizeof(float2);
         const int64_t ntx = (p.n[0] + SC - 1) / SC, nta = (p.n[p.axis] + SO - 1) / SO;
@@ -438,7 +505,7 @@ bool tiled_pass_supported(const TiledPassParams& p)
     // extents (a channel axis) keep the general kernel
     if (p.n[0] < (p.axis == 0 ? 16 : 32)) return false;
     // the staged window of the widest kernel must fit one CTA's shared memory
-    const size_t smx = ((size_t)XR * x_pitch(p.ntap) + p.ntap + 3) * 4;
+    const size_t smx = (2 * (size_t)XR * x_pitch(p.ntap) + p.ntap + 3) * 4;
     const size_t sms = 2 * (size_t)s_rows(p.ntap) * SC * 4 + (size_t)(p.ntap + 1) * 8;
     if (smx > 200 * 1024 || sms > 200 * 1024) return false;
     return true;
