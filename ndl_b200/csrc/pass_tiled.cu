@@ -19,6 +19,7 @@
 // summed.  Taps are the pass's dense offsets omin .. omin+K-1 in ascending
 // order.
 #include <algorithm>
+#include <atomic>
 
 #include "dtype.cuh"
 
@@ -429,6 +430,48 @@ __global__ void __launch_bounds__(NT, 4) k_tpass_s(const __grid_constant__ Tiled
     cp_async_wait<0>();
 }
 
+// The SM count of the current device (cached per device).
+int sm_count()
+{
+    static std::atomic<int> cache[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) dev = 0;
+    int n = cache[dev].load(std::memory_order_relaxed);
+    if (n == 0) {
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1) n = 148;
+        cache[dev].store(n, std::memory_order_relaxed);
+    }
+    return n;
+}
+
+// The persistent grid of a pass kernel (as many CTAs as fit at once, at most
+// one per tile) and its dynamic shared-memory opt-in, each looked up once per
+// kernel and tap count: the plain path launches these passes once per call,
+// and the queries would otherwise cost host time on every launch.
+template <class Kern>
+cudaError_t persistent_grid(Kern kern, size_t smem, int K, int64_t ntiles, int64_t* grid)
+{
+    static std::atomic<int> smem_set{0};
+    static std::atomic<int> per_sm_k[kMaxTaps + 1];
+    if (smem > 48 * 1024 && (int)smem > smem_set.load(std::memory_order_relaxed)) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        int cur = smem_set.load(std::memory_order_relaxed);
+        while ((int)smem > cur && !smem_set.compare_exchange_weak(cur, (int)smem)) {
+        }
+    }
+    const int k = K < 0 ? 0 : (K > kMaxTaps ? kMaxTaps : K);
+    int per_sm = per_sm_k[k].load(std::memory_order_relaxed);
+    if (per_sm == 0) {
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem) != cudaSuccess || per_sm < 1)
+            per_sm = 1;
+        per_sm_k[k].store(per_sm, std::memory_order_relaxed);
+    }
+    *grid = std::min<int64_t>(ntiles, (int64_t)sm_count() * per_sm);
+    return cudaSuccess;
+}
+
 template <class Tin, class Tout>
 cudaError_t launch_t(const TiledPassParams& p_in, cudaStream_t s)
 {
@@ -442,17 +485,9 @@ cudaError_t launch_t(const TiledPassParams& p_in, cudaStream_t s)
         const int64_t ntiles = ntx * ((p.rows + XR - 1) / XR);
         if (ntiles > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
         auto kern = k_tpass_x<Tin, Tout>;
-        if (smem > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e != cudaSuccess) return e;
-        }
-        // persistent CTAs: as many as fit at once
-        int dev = 0, sms = 148, per_sm = 1;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem);
-        if (per_sm < 1) per_sm = 1;
-        const int64_t grid = std::min<int64_t>(ntiles, (int64_t)sms * per_sm);
+        int64_t grid = 0;
+        cudaError_t e = persistent_grid(kern, smem, K, ntiles, &grid);
+        if (e != cudaSuccess) return e;
         kern<<<(unsigned)grid, NT, smem, s>>>(p, (uint32_t)ntiles);
     } else {
         const size_t smem = 2 * (size_t)s_rows(K) * SC * sizeof(float) + (size_t)((K + 1) & ~1) * sizeof(float2);
@@ -462,17 +497,9 @@ cudaError_t launch_t(const TiledPassParams& p_in, cudaStream_t s)
         if (ntiles > 0x7fffffffLL || ntx * nta > 0xffffffffLL) return cudaErrorInvalidConfiguration;
         p.dta.init((uint32_t)nta);
         auto kern = k_tpass_s<Tin, Tout>;
-        if (smem > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e != cudaSuccess) return e;
-        }
-        // persistent CTAs: as many as fit at once
-        int dev = 0, sms = 148, per_sm = 1;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem);
-        if (per_sm < 1) per_sm = 1;
-        const int64_t grid = std::min<int64_t>(ntiles, (int64_t)sms * per_sm);
+        int64_t grid = 0;
+        cudaError_t e = persistent_grid(kern, smem, K, ntiles, &grid);
+        if (e != cudaSuccess) return e;
         kern<<<(unsigned)grid, NT, smem, s>>>(p, (uint32_t)ntiles);
     }
     count_launch();
