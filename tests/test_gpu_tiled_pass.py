@@ -4,7 +4,7 @@ against the FP64 oracle.
 They run the plain path's passes where no fused kernel is compiled: Gaussians
 wider than the fused widths (volumes above 19 taps, images above 25), uneven
 per-axis widths, four-axis chains, strided and mirrored views, 16-bit
-storage.  Bounds are relative to the stencil magnitude (the same chain on
+storage, and more outer lines than a launch grid's second dimension holds.  Bounds are relative to the stencil magnitude (the same chain on
 |x| and |w|): FP32 1e-6; 16-bit storage 4e-3 (FP32 intermediates, one
 rounding at the end).
 """
@@ -100,3 +100,20 @@ def test_wide_gaussian_16bit_storage(tdt):
     w = O.gaussian_weights(5.0)
     # FP32 intermediates, one rounding to 16 bits at the end
     _check(o.tensor().float().cpu().numpy(), xd, [(a, w) for a in range(3)], BorderMode.Reflect, 4e-3)
+
+
+@pytest.mark.parametrize("border", [BorderMode.Clamp, BorderMode.Reflect])
+def test_strided_pass_many_outer_lines(border):
+    # a pass along an axis of extent 2 whose outer index (the other axes but
+    # x) runs past 65535 lines, and odd row counts for the x pass: the
+    # persistent tile walk's index decomposition
+    rng = np.random.default_rng(100 + int(border))
+    x = rng.standard_normal((300, 301, 2, 33)).astype(np.float32)     # (w, z, y, x)
+    passes = []
+    for ax, k in ((0, 5), (1, 3), (2, 7), (3, 3)):
+        w = rng.standard_normal(k)
+        passes.append((ax, w / np.abs(w).sum()))
+    s = Image.from_tensor(torch.from_numpy(x).to(DEV))
+    o = Image.empty(s.extent(), torch.float32)
+    n.convolve_axes(s, o, passes, border)
+    _check(o.tensor().cpu().numpy(), x, passes, border, 1e-6)
