@@ -483,7 +483,7 @@ def dog_form(g, it, hbm):
 
 
 def other_forms(args, hbm):
-    """The other BASELINE configurations, timed briefly (each > L2)."""
+    """The other workloads (configurations 1, 2, 4 and 5 and the further forms), timed briefly (each > L2)."""
     import torch
 
     import ndl_b200 as n

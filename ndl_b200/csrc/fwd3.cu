@@ -433,9 +433,9 @@ __global__ void __launch_bounds__(NT, Occ3<KZ>::value)
         }
         stage_next = (stage_next + 1 == STAGES) ? 0 : stage_next + 1;
 
-        // Y pass: round 0, warp w = row quad w, lane = column pair (the
-        // first 64 of the YC columns); round 1, the last 2 HX columns' pairs,
-        // by the first 4 HX threads
+        // Y pass: first sweep, warp w = row quad w, lane = column pair (the
+        // first 64 of the YC columns); second sweep, the last 2 HX columns'
+        // pairs, by the first 4 HX threads
         const Tin* sb = s_in + stage * G::STAGE + G::D;
 #pragma unroll
         for (int i = 0; i < 2; i++) {
